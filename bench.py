@@ -1,0 +1,337 @@
+#!/usr/bin/env python3
+"""Benchmark: batched SrOH steady-state force maps (the batched-map workload).
+
+Workload (per GPU, weak scaling): 4096 seeded parameter sets (4 detunings
+U[-40, 0] MHz added to the SrOH transition references, per-frequency s0
+log-uniform in [0.1, 10], B' U[5, 40] G/cm), each a 256 x 256 grid of
+v in [-10, 10] m/s and z in [-10, 10] mm: 2.68e8 steady-state force
+evaluations per step.  Synthetic inputs of exactly that shape (seed 20261203
++ rank).
+
+value      : force evaluations/s of the FP32-bulk + FP64-LU + refinement form,
+             inputs resident, device-timed (CUDA events), max over ranks.
+plain_fp64 : the same for the plain FP64 form on the same grid.
+e2e        : the same metric through the public API with host arrays: per step
+             the parameter sets and grid axes go host->device and the force
+             map comes back device->host (inside the timed region).
+roofline   : the force kernel against the measured FP64/FP32 FMA peaks of
+             this GPU (mm_peak_probe); algorithmic FLOPs per point from
+             molmot_b200/flops.py.
+cpu_baseline: the reference's numba core restated (oracle/rate_eq_numba.py)
+             on all host cores, on a bounded sample of the same workload.
+
+`--impl reference` prints the CPU reference arm instead (rank 0 only).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "16-level steady-state force evals/s and particle-steps/s: plain FP64 vs FP32+refine @1e-6"
+N_SETS, NV, NZ = 4096, 256, 256
+SEED = 20261203
+
+
+def make_params(mol, n_sets, seed):
+    rng = np.random.default_rng(seed)
+    E = mol.energies
+    ref = np.array([E[15] - E[0], E[15] - E[0], E[15] - E[9], E[15] - E[9]])
+    det = rng.uniform(-40e6, 0.0, (n_sets, 4))
+    s0 = 10 ** rng.uniform(-1, 1, (n_sets, 4))
+    B = rng.uniform(5, 40, n_sets) * 1e-2
+    pols = np.array([2, 0, 2, 0])
+    kdir = np.tile([1.0, -1.0], (n_sets, 4))
+    freq = np.repeat(ref[None, :] + det, 2, axis=1)
+    pol = np.tile(np.stack([pols, 2 - pols], 1).ravel(), (n_sets, 1)).astype(np.int32)
+    s0b = np.repeat(s0, 2, axis=1)
+    return kdir, freq, pol, s0b, B
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.gpu)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, f[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peak_probe(torch):
+    """Measured FP64 and FP32 FMA throughput (TFLOP/s) of this GPU."""
+    import ctypes
+    from molmot_b200 import _lib
+    L = _lib.load()
+    out = {}
+    for which, name, iters in [(0, "fp64", 4096), (1, "fp32", 16384)]:
+        best = 0.0
+        for _ in range(3):
+            ms, fl = ctypes.c_double(), ctypes.c_double()
+            _lib.check(L.mm_peak_probe(which, iters, ctypes.byref(ms), ctypes.byref(fl),
+                                       ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)),
+                       "mm_peak_probe")
+            best = max(best, fl.value / (ms.value * 1e-3) / 1e12)
+        out[name] = best
+    return out
+
+
+def cpu_baseline(mol, n_sets_sample=8):
+    """The reference's numba core (restated) on all host cores, on a sample."""
+    from oracle import rate_eq_numba as nb
+    kdir, freq, pol, s0, B = make_params(mol, n_sets_sample, SEED)
+    v = np.linspace(-10, 10, NV)
+    z = np.linspace(-1e-2, 1e-2, NZ)
+    nb.force_grid(mol, kdir[:1], freq[:1], pol[:1], s0[:1], B[:1], v[:4], z[:4])  # compile
+    t0 = time.perf_counter()
+    nb.force_grid(mol, kdir, freq, pol, s0, B, v, z)
+    dt = time.perf_counter() - t0
+    n = n_sets_sample * NV * NZ
+    return {"value": n / dt, "unit": "force evals/s", "cores": nb.threads(), "kind": "port",
+            "sample": f"{n_sets_sample} of the {N_SETS} parameter sets, full {NV}x{NZ} grid "
+                      f"({n} points, {dt:.2f} s), numba restatement of _rate_eq_core, "
+                      f"prange over points, os.cpu_count()={os.cpu_count()}"}
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from molmot_b200.molecules import load_sroh_from_julia
+    from oracle import rate_eq_numba as nb
+    mol = load_sroh_from_julia()
+    n_sample = 4
+    kdir, freq, pol, s0, B = make_params(mol, n_sample, SEED)
+    v = np.linspace(-10, 10, NV)
+    z = np.linspace(-1e-2, 1e-2, NZ)
+    nb.force_grid(mol, kdir[:1], freq[:1], pol[:1], s0[:1], B[:1], v[:4], z[:4])
+    for _ in range(args.warmup):
+        nb.force_grid(mol, kdir, freq, pol, s0, B, v, z)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        nb.force_grid(mol, kdir, freq, pol, s0, B, v, z)
+        times.append(time.perf_counter() - t0)
+    n = n_sample * NV * NZ
+    val = n / (sum(times) / len(times))
+    sample = (f"each step: {n_sample} of the {N_SETS} parameter sets x full {NV}x{NZ} grid "
+              f"({n} points) on the host CPU")
+    line = {"impl": "reference", "metric": METRIC, "value": val, "unit": "force evals/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"SrOH batched force maps, {N_SETS} sets x {NV}x{NZ} (v,z) grid, "
+                                   "8-beam DC MOT (bounded CPU sample per step)",
+                       "sets_per_step_sample": n_sample},
+            "cpu_baseline": {"value": val, "unit": "force evals/s", "cores": nb.threads(),
+                             "kind": "port", "sample": sample},
+            "e2e": {"value": val, "unit": "force evals/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--sets", type=int, default=N_SETS, help="parameter sets per GPU")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import torch
+    import torch.distributed as dist
+    from molmot_b200.molecules import load_sroh_from_julia
+    from molmot_b200.engine import MoleculePack, BeamSets, force_batch
+    from molmot_b200.flops import active_triples, flops_per_point
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    dev = torch.device("cuda", local)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    mol = load_sroh_from_julia()
+    pack = MoleculePack(mol)
+    n_sets = args.sets
+    kdir, freq, pol, s0, B = make_params(mol, n_sets, SEED + rank)
+    v_h = np.linspace(-10, 10, NV)
+    z_h = np.linspace(-1e-2, 1e-2, NZ)
+    bs = BeamSets(kdir, freq, pol, s0, B)
+    v_d = torch.as_tensor(v_h, device=dev)
+    z_d = torch.as_tensor(z_h, device=dev)
+    n_pts = n_sets * NV * NZ
+    out = {"F": torch.empty((n_sets, NV, NZ), dtype=torch.float64, device=dev)}
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > L2 (126 MB)
+
+    def timed(precision, steps, warmup):
+        for _ in range(warmup):
+            force_batch(pack, bs, v_d, z_d, grid=True, precision=precision, out=out)
+        barrier()
+        evs = []
+        for _ in range(steps):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            force_batch(pack, bs, v_d, z_d, grid=True, precision=precision, out=out)
+            e1.record()
+            evs.append((e0, e1))
+        barrier()
+        ms = sum(a.elapsed_time(b) for a, b in evs) / steps
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    peaks = peak_probe(torch)
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms32 = timed("fp32", args.steps, args.warmup)
+    ms64 = timed("fp64", args.steps, args.warmup)
+    clk = clocks.stop()
+
+    # end to end through the public API with host buffers
+    pinned_F = torch.empty((n_sets, NV, NZ), dtype=torch.float64, pin_memory=True)
+    params_h = [np.ascontiguousarray(a) for a in (kdir, freq, pol, s0, B)]
+    h2d = sum(a.nbytes for a in params_h) + v_h.nbytes + z_h.nbytes
+    d2h = pinned_F.numel() * 8
+
+    def e2e_step():
+        b2 = BeamSets(*params_h)
+        vv = torch.as_tensor(v_h).to(dev, non_blocking=True)
+        zz = torch.as_tensor(z_h).to(dev, non_blocking=True)
+        o = force_batch(pack, b2, vv, zz, grid=True, precision="fp32", want_pop=False,
+                        want_R=False, want_status=False)
+        pinned_F.copy_(o["F"], non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        return pinned_F
+
+    for _ in range(max(1, args.warmup)):
+        e2e_step()
+    barrier()
+    e2e_ms = []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e2e_step()
+        e2e_ms.append(1e3 * (time.perf_counter() - t0))
+    t = torch.tensor([sum(e2e_ms) / len(e2e_ms)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_e2e = float(t.item())
+
+    A = active_triples(mol.d_squared, pol[0])
+    f64_32, f32_32 = flops_per_point(12, 4, 8, A, refine=True)
+    f64_64, _ = flops_per_point(12, 4, 8, A, refine=False)
+    # FP32 form: FP64 and FP32 pipes run concurrently; the bound is the slower of the two
+    t_min32 = max(f64_32 * n_pts / (peaks["fp64"] * 1e12), f32_32 * n_pts / (peaks["fp32"] * 1e12))
+    achieved32 = (f64_32 + f32_32) * n_pts / (ms32 * 1e-3) / 1e12
+    peak32 = (f64_32 + f32_32) * n_pts / t_min32 / 1e12
+    achieved64 = f64_64 * n_pts / (ms64 * 1e-3) / 1e12
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(mol)
+
+    if rank == 0:
+        total = n_pts * world
+        line = {
+            "metric": METRIC, "value": total / (ms32 * 1e-3), "unit": "force evals/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms32,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+            "data": "synthetic",
+            "config": {"workload": f"SrOH (12 ground + 4 excited) batched force maps: {n_sets} "
+                                   f"parameter sets x {NV}x{NZ} (v, z) grid per GPU, 8-beam DC MOT, "
+                                   "FP32 rates + FP64 LU + 1 refinement step",
+                       "points_per_step_per_gpu": n_pts, "parallelism": f"sets sharded, {world} GPU(s)",
+                       "l2": "256 MB buffer written between timed steps (> 126 MB L2)"},
+            "plain_fp64": {"value": total / (ms64 * 1e-3), "unit": "force evals/s",
+                           "ms_per_step": ms64, "ratio_fp32_over_fp64": ms64 / ms32,
+                           "roofline": {"bound": "fp64", "achieved": achieved64,
+                                        "peak": peaks["fp64"], "unit": "TFLOP/s",
+                                        "frac": achieved64 / peaks["fp64"]}},
+            "roofline": {"bound": "fp64+fp32", "achieved": achieved32, "peak": peak32,
+                         "unit": "TFLOP/s", "frac": achieved32 / peak32, "traffic": None,
+                         "peak_source": "mm_peak_probe FMA loop on this GPU: "
+                                        f"fp64 {peaks['fp64']:.2f}, fp32 {peaks['fp32']:.2f} TFLOP/s",
+                         "flops_per_point": {"fp64": f64_32, "fp32": f32_32}},
+            "e2e": {"value": total / (ms_e2e * 1e-3), "unit": "force evals/s",
+                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                    "ms_per_step": ms_e2e},
+            "gpu_launches": args.steps * 2,
+            "clocks": clk,
+        }
+        if cpu is not None:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,150 @@
+/*
+ * molmot_b200.h -- C ABI of the B200 rate-equation steady-state force library.
+ *
+ * Plain C: opaque handles, plain pointers and sizes, integer return codes.
+ * All array arguments of the compute calls are DEVICE pointers owned by the
+ * caller; `stream` is a cudaStream_t passed as void* (NULL = legacy default
+ * stream).  Calls are stream-ordered and do not synchronise the host unless
+ * stated.  Handles are immutable after creation and may be shared between
+ * host threads.
+ *
+ * Return codes: 0 ok; < 0 argument or CUDA error (see mm_last_error()).
+ * Per-point numerical conditions go to the optional status array
+ * (bit 1: a pivot below 1e-30 was skipped, bit 2: non-finite result,
+ *  bit 4: every population clamped to zero).
+ *
+ * Each entry point names the reference interface it replaces (paths within
+ * the molmot project).
+ */
+#ifndef MOLMOT_B200_H
+#define MOLMOT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define MM_API __attribute__((visibility("default")))
+#else
+#define MM_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MM_MAX_GROUND 48
+#define MM_MAX_EXCITED 16
+#define MM_MAX_BEAMS 32
+
+/* precision of the force kernels */
+#define MM_PREC_FP64 0         /* plain FP64, reference operation order */
+#define MM_PREC_FP32_REFINE 1  /* FP32 rates/shifts/reductions, FP64 LU + 1 refinement step */
+
+/* point layouts of mm_force_batch */
+#define MM_LAYOUT_POINTS 0 /* v[i], z[i]; point i belongs to set i / points_per_set */
+#define MM_LAYOUT_GRID 1   /* per set the outer product v[nv] x z[nz], index (set*nv+iv)*nz+iz */
+
+typedef struct mm_pack mm_pack;
+typedef struct mm_beams mm_beams;
+
+/* Molecule description (host pointers, copied by mm_pack_create).
+ * Replaces molmot/molecules/sroh.py:87-174 MolecularData as consumed by
+ * molmot_cuda/rate_equations_cuda.py:399-441 CUDAMolData. */
+typedef struct {
+    int32_t n_ground, n_excited;
+    const double *energies;      /* [n_g + n_e] Hz                                 */
+    const double *d_squared;     /* [n_g][n_e][3] |tdm|^2, q = sigma-, pi, sigma+   */
+    const double *zeeman_z_diag; /* [n_g + n_e] Zeeman diagonal (Gamma/2pi per G)  */
+    double Gamma;                /* rad/s                                          */
+    double k;                    /* 1/m                                            */
+    double mass;                 /* kg                                             */
+    /* 3D model only (may be NULL for 1D use): ground Zeeman blocks and |tdm| */
+    const double *zeeman_ground_re; /* [3][n_g][n_g] x, y, z real parts          */
+    const double *zeeman_ground_im; /* [3][n_g][n_g] imaginary parts             */
+    const double *zeeman_excited_z; /* [n_e] Re diag of zeeman_z excited block   */
+    const double *tdm_abs;          /* [n_g][n_e][3] |tdm[g, n_g+e, q]|          */
+} mm_mol_desc;
+
+/* Parameter sets of beams (host pointers, copied by mm_beams_create).
+ * Each of n_sets sets has n_beams beams.  Replaces the LaserBeam lists of
+ * molmot/obe/fields.py:22-58 (kdir_z, freq_offset, polarization, s0) plus
+ * the per-call B_gradient of molmot/obe/rate_equations_jit.py:148. */
+typedef struct {
+    int32_t n_beams;
+    const double *kdir;       /* [n_sets][n_beams] z-projection of k (1D)          */
+    const double *freq;       /* [n_sets][n_beams] absolute frequency, Hz          */
+    const int32_t *pol;       /* [n_sets][n_beams] 0, 1, 2                         */
+    const double *s0;         /* [n_sets][n_beams] saturation parameter            */
+    const double *b_gradient; /* [n_sets] T/m                                      */
+    double gamma_eff;         /* Gamma_eff_factor (same for all sets)              */
+    /* 3D model only (may be NULL): unit k vectors and 1/e^2 radii (<= 0: plane wave) */
+    const double *khat;       /* [n_sets][n_beams][3]                              */
+    const double *radius;     /* [n_sets][n_beams]                                 */
+} mm_beam_desc;
+
+typedef struct {
+    int32_t precision;        /* MM_PREC_*                                         */
+    int32_t layout;           /* MM_LAYOUT_*                                       */
+    int64_t points_per_set;   /* MM_LAYOUT_POINTS                                  */
+    int64_t nv, nz;           /* MM_LAYOUT_GRID                                    */
+    double hbar;              /* J s; <= 0 selects 1.0545718e-34 (the JIT value)   */
+    int32_t uniform_fallback; /* 1: p = 1/n_g when every population clamps to 0
+                                 (reference CUDA / Python); 0: keep zeros (JIT)   */
+    int32_t reserved;
+} mm_batch_opts;
+
+/* Last error message of the calling host thread ("" if none). */
+MM_API const char *mm_last_error(void);
+
+/* Library version string. */
+MM_API const char *mm_version(void);
+
+/* Upload a molecule; replaces CUDAMolData molecule transfer
+ * (molmot_cuda/rate_equations_cuda.py:399-441). */
+MM_API int mm_pack_create(const mm_mol_desc *desc, mm_pack **out);
+MM_API int mm_pack_destroy(mm_pack *pack);
+
+/* Upload n_sets parameter sets of beams; replaces CUDAMolData beam transfer
+ * (molmot_cuda/rate_equations_cuda.py:370-397, 427-441). */
+MM_API int mm_beams_create(const mm_beam_desc *desc, int32_t n_sets, mm_beams **out);
+MM_API int mm_beams_destroy(mm_beams *beams);
+
+/*
+ * Steady-state force, populations and scattering rate for a batch of points.
+ * Replaces solve_rate_equations_batch (molmot_cuda/rate_equations_cuda.py:448-544,
+ * kernel :51-277) and, point by point, _rate_eq_core
+ * (molmot/obe/rate_equations_jit.py:18-145).
+ * v, z: device arrays (layout per opts).  Outputs: F[n], R[n] (R nullable),
+ * pop[n][n_ground] (nullable), status[n] (nullable), n = total points.
+ */
+MM_API int mm_force_batch(const mm_pack *pack, const mm_beams *beams, const double *v,
+                   const double *z, int64_t n_points, const mm_batch_opts *opts,
+                   double *F, double *R, double *pop, int32_t *status, void *stream);
+
+/*
+ * N independent 1D trajectories with symplectic Euler, one beam set (set 0).
+ * Replaces traj_kernel / simulate_trajectories_cuda
+ * (molmot_cuda/trajectories_cuda.py:44-280, 305-426) and
+ * _trajectory_1d_jit (molmot/propagation/trajectories_jit.py:18-58).
+ * z_traj / v_traj: [N][n_steps] or NULL.  n_actual: [N] steps run.
+ */
+MM_API int mm_traj1d_run(const mm_pack *pack, const mm_beams *beams, const double *z0,
+                  const double *v0, int64_t n_particles, double dt, int64_t n_steps,
+                  double z_escape, const mm_batch_opts *opts, double *z_final,
+                  double *v_final, int32_t *n_actual, double *z_traj, double *v_traj,
+                  void *stream);
+
+/*
+ * FMA-throughput probe (measurement aid; no counterpart in the reference).
+ * which = 0: FP64, 1: FP32.  Runs a register-only FMA loop on every SM and
+ * writes its duration (ms) and FLOP count (2 per FMA); synchronises `stream`.
+ * Used as the roofline peak of the force kernels, which are bound by the
+ * FP64/FP32 CUDA-core pipes.
+ */
+MM_API int mm_peak_probe(int32_t which, int64_t iters, double *ms_out, double *flops_out,
+                         void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MOLMOT_B200_H */

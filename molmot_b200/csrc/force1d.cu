@@ -1,0 +1,300 @@
+// force1d.cu -- batched 1D steady-state force and fused 1D trajectory
+// kernels, and their C-ABI entry points (mm_force_batch, mm_traj1d_run).
+//
+// One CTA works on one parameter set: its prologue stages the molecule and
+// the set's beams into shared memory and compacts the active
+// (ground, beam, excited) triples; then groups of G lanes stream over the
+// set's points.  The trajectory kernel gives each group one particle and
+// runs the whole Euler loop in registers.
+#include <stdio.h>
+#include <algorithm>
+#include "rate_core.cuh"
+
+namespace {
+
+constexpr int kThreads = 128;
+
+template <int NGMAX, int NEMAX, int G, bool FP32>
+__global__ void __launch_bounds__(kThreads)
+force_kernel(ForceParams P)
+{
+    using GS = GroupShape<NGMAX, NEMAX, G>;
+    extern __shared__ __align__(16) unsigned char sm[];
+    SmemLayout Ly;
+    const int ngroups = kThreads / G;
+    Ly.build(P.n_g, P.n_e, P.n_b, GS::CPL, ngroups, FP32);
+    const long long pts_per_set = (P.layout == MM_LAYOUT_GRID) ? P.nv * P.nz : P.pps;
+
+    const int lane = threadIdx.x & 31, t = lane % G, gbase = lane - t;
+    const int group = threadIdx.x / G;
+    double *scr = (double *)(sm + Ly.scratch) + (size_t)group * Ly.scratch_per_group;
+    double *fd = scr, *Ese = scr + P.n_b;
+
+    for (int set = blockIdx.y; set < P.n_sets; set += gridDim.y) {
+        const long long set_first = (long long)set * pts_per_set;
+        long long set_count = pts_per_set;
+        if (set_first + set_count > P.n_points) set_count = P.n_points - set_first;
+        if (set_count <= 0) continue;  // uniform over the CTA
+        SetView S;
+        __syncthreads();
+        build_set_tables<G, GS::CPL, FP32>(P, set, sm, Ly, S);
+        const double Bg = P.bgrad[set];
+        const long long chunk = (set_count + gridDim.x - 1) / gridDim.x;
+        const long long start = (long long)blockIdx.x * chunk;
+        const long long end = min(start + chunk, set_count);
+        for (long long base = start; base < end; base += ngroups) {
+            const long long ip = base + group;
+            const bool valid = ip < end;
+            const long long ipc = valid ? ip : start;
+            double v, z;
+            if (P.layout == MM_LAYOUT_GRID) {
+                v = P.v[ipc / P.nz];
+                z = P.z[ipc % P.nz];
+            } else {
+                v = P.v[set_first + ipc];
+                z = P.z[set_first + ipc];
+            }
+            double xs[GS::CPL];
+            const PointOut o = solve_point<NGMAX, NEMAX, G, FP32>(P, S, fd, Ese, t, gbase, v, z, Bg, xs);
+            if (valid) {
+                const long long gi = set_first + ip;
+                if (t == 0) {
+                    P.F[gi] = o.F;
+                    if (P.R) P.R[gi] = o.R;
+                    if (P.status) P.status[gi] = o.status;
+                }
+                if (P.pop) {
+#pragma unroll
+                    for (int c = 0; c < GS::CPL; c++) {
+                        const int k = c * G + t;
+                        if (k < P.n_g) P.pop[gi * P.n_g + k] = xs[c];
+                    }
+                }
+            }
+        }
+    }
+}
+
+struct TrajParams {
+    double dt, z_escape, mass;
+    long long n_particles, n_steps;
+    const double *z0, *v0;
+    double *z_final, *v_final, *z_traj, *v_traj;
+    int32_t *n_actual;
+};
+
+// Fused 1D Euler trajectories (molmot/propagation/trajectories_jit.py:18-58):
+// v_j = v_{j-1} + F(v_{j-1}, z_{j-1})/m dt; z_j = z_{j-1} + v_j dt; stop when |z| > z_escape.
+template <int NGMAX, int NEMAX, int G, bool FP32>
+__global__ void __launch_bounds__(kThreads)
+traj1d_kernel(ForceParams P, TrajParams T)
+{
+    using GS = GroupShape<NGMAX, NEMAX, G>;
+    extern __shared__ __align__(16) unsigned char sm[];
+    SmemLayout Ly;
+    const int ngroups = kThreads / G;
+    Ly.build(P.n_g, P.n_e, P.n_b, GS::CPL, ngroups, FP32);
+    const int lane = threadIdx.x & 31, t = lane % G, gbase = lane - t;
+    const int group = threadIdx.x / G;
+    double *scr = (double *)(sm + Ly.scratch) + (size_t)group * Ly.scratch_per_group;
+    double *fd = scr, *Ese = scr + P.n_b;
+    SetView S;
+    build_set_tables<G, GS::CPL, FP32>(P, 0, sm, Ly, S);
+    const double Bg = P.bgrad[0];
+
+    const long long ip = (long long)blockIdx.x * ngroups + group;
+    const bool valid = ip < T.n_particles;
+    double z = valid ? T.z0[ip] : 0.0, v = valid ? T.v0[ip] : 0.0;
+    long long na = T.n_steps;
+    bool done = !valid;
+    if (valid && T.z_traj && t == 0) { T.z_traj[ip * T.n_steps] = z; T.v_traj[ip * T.n_steps] = v; }
+    for (long long j = 1; j < T.n_steps; j++) {
+        if (__all_sync(0xffffffffu, done)) break;
+        double xs[GS::CPL];
+        const PointOut o = solve_point<NGMAX, NEMAX, G, FP32>(P, S, fd, Ese, t, gbase, v, z, Bg, xs);
+        if (!done) {
+            const double a = o.F / T.mass;
+            v = v + a * T.dt;
+            z = z + v * T.dt;
+            if (T.z_traj && t == 0) { T.z_traj[ip * T.n_steps + j] = z; T.v_traj[ip * T.n_steps + j] = v; }
+            if (fabs(z) > T.z_escape) {
+                na = j;
+                done = true;
+                if (T.z_traj && t == 0)
+                    for (long long s = j + 1; s < T.n_steps; s++) {
+                        T.z_traj[ip * T.n_steps + s] = z;
+                        T.v_traj[ip * T.n_steps + s] = v;
+                    }
+            }
+        }
+    }
+    if (valid && t == 0) {
+        T.z_final[ip] = z;
+        T.v_final[ip] = v;
+        T.n_actual[ip] = (int32_t)na;
+    }
+}
+
+// Size classes: (NGMAX, NEMAX, G).
+template <int NGMAX, int NEMAX, int G>
+struct Class {
+    static constexpr int ng = NGMAX, ne = NEMAX, g = G;
+};
+
+template <class C, bool FP32>
+size_t smem_bytes(const ForceParams &P)
+{
+    SmemLayout Ly;
+    Ly.build(P.n_g, P.n_e, P.n_b, GroupShape<C::ng, C::ne, C::g>::CPL, kThreads / C::g, FP32);
+    return Ly.total;
+}
+
+template <class C, bool FP32>
+int launch_force(const ForceParams &P, long long pts_per_set, cudaStream_t st)
+{
+    auto kern = force_kernel<C::ng, C::ne, C::g, FP32>;
+    const size_t sb = smem_bytes<C, FP32>(P);
+    if (sb > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb);
+        if (mm_cuda_check(e, "cudaFuncSetAttribute")) return -3;
+    }
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    int per_sm = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, sb);
+    if (per_sm < 1) per_sm = 1;
+    const int ngroups = kThreads / C::g;
+    // enough CTAs per set to fill the GPU a few times over, at least 64 points per group
+    const long long want = (long long)nsm * per_sm * 4;
+    long long gx = std::max<long long>(1, want / std::max(1, P.n_sets));
+    const long long max_gx = std::max<long long>(1, (pts_per_set + (long long)ngroups * 64 - 1) /
+                                                      ((long long)ngroups * 64));
+    gx = std::min(gx, max_gx);
+    gx = std::min<long long>(gx, 1 << 20);
+    const int gy = std::min(P.n_sets, 65535);
+    dim3 grid((unsigned)gx, (unsigned)gy);
+    kern<<<grid, kThreads, sb, st>>>(P);
+    return mm_cuda_check(cudaGetLastError(), "force_kernel launch") ? -3 : 0;
+}
+
+template <class C, bool FP32>
+int launch_traj(const ForceParams &P, const TrajParams &T, cudaStream_t st)
+{
+    auto kern = traj1d_kernel<C::ng, C::ne, C::g, FP32>;
+    const size_t sb = smem_bytes<C, FP32>(P);
+    if (sb > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb);
+        if (mm_cuda_check(e, "cudaFuncSetAttribute")) return -3;
+    }
+    const int ngroups = kThreads / C::g;
+    const long long gx = (T.n_particles + ngroups - 1) / ngroups;
+    kern<<<(unsigned)gx, kThreads, sb, st>>>(P, T);
+    return mm_cuda_check(cudaGetLastError(), "traj1d_kernel launch") ? -3 : 0;
+}
+
+// Size-class dispatch.  SrOH (12 ground, 4 excited) has an exact class.
+template <class F>
+int dispatch_class(int n_g, int n_e, F &&f)
+{
+    if (n_g <= 12 && n_e <= 4) return f(Class<12, 4, 4>{});
+    mm_set_error("molecule size n_ground=%d n_excited=%d exceeds the register-resident 1D "
+                 "kernel class (n_ground <= 12, n_excited <= 4)", n_g, n_e);
+    return -1;
+}
+
+int fill_params(const mm_pack *pack, const mm_beams *beams, const mm_batch_opts *opts,
+                ForceParams &P)
+{
+    if (!pack || !beams) { mm_set_error("null pack or beams handle"); return -1; }
+    if (beams->n_b < 1 || beams->n_b > MM_MAX_BEAMS) {
+        mm_set_error("n_beams=%d out of range [1, %d]", beams->n_b, MM_MAX_BEAMS);
+        return -1;
+    }
+    P.n_g = pack->n_g; P.n_e = pack->n_e; P.n_b = beams->n_b; P.n_sets = beams->n_sets;
+    P.Gamma = pack->Gamma; P.k = pack->k;
+    P.hbar = (opts && opts->hbar > 0) ? opts->hbar : MM_HBAR_JIT;
+    P.geff = beams->gamma_eff;
+    P.E = pack->buf + pack->oE; P.zd = pack->buf + pack->ozd;
+    P.d2 = pack->buf + pack->od2; P.BR = pack->buf + pack->oBR;
+    P.kdir = beams->kdir; P.freq = beams->freq; P.s0 = beams->s0; P.bgrad = beams->bgrad;
+    P.pol = beams->pol;
+    P.uniform_fb = opts ? opts->uniform_fallback : 0;
+    return 0;
+}
+
+}  // namespace
+
+extern "C" int mm_force_batch(const mm_pack *pack, const mm_beams *beams, const double *v,
+                              const double *z, int64_t n_points, const mm_batch_opts *opts,
+                              double *F, double *R, double *pop, int32_t *status, void *stream)
+{
+    ForceParams P;
+    if (fill_params(pack, beams, opts, P)) return -1;
+    if (!opts) { mm_set_error("opts is required"); return -1; }
+    if (!v || !z || !F) { mm_set_error("v, z and F must be non-null"); return -1; }
+    if (n_points < 0) { mm_set_error("n_points < 0"); return -1; }
+    if (n_points == 0) return 0;
+    P.layout = opts->layout;
+    P.nv = opts->nv; P.nz = opts->nz; P.pps = opts->points_per_set;
+    long long pps;
+    if (opts->layout == MM_LAYOUT_GRID) {
+        if (opts->nv < 1 || opts->nz < 1) { mm_set_error("grid layout needs nv, nz >= 1"); return -1; }
+        pps = opts->nv * opts->nz;
+        if (n_points != pps * (long long)beams->n_sets) {
+            mm_set_error("grid layout: n_points=%lld != n_sets*nv*nz=%lld", (long long)n_points,
+                         pps * (long long)beams->n_sets);
+            return -1;
+        }
+    } else if (opts->layout == MM_LAYOUT_POINTS) {
+        pps = opts->points_per_set > 0 ? opts->points_per_set : n_points;
+        P.pps = pps;
+        if ((n_points + pps - 1) / pps > beams->n_sets) {
+            mm_set_error("points layout: %lld points at %lld per set need more than %d sets",
+                         (long long)n_points, pps, beams->n_sets);
+            return -1;
+        }
+    } else {
+        mm_set_error("unknown layout %d", opts->layout);
+        return -1;
+    }
+    P.n_points = n_points;
+    P.v = v; P.z = z; P.F = F; P.R = R; P.pop = pop; P.status = status;
+    const bool fp32 = opts->precision == MM_PREC_FP32_REFINE;
+    if (opts->precision != MM_PREC_FP64 && !fp32) { mm_set_error("unknown precision %d", opts->precision); return -1; }
+    cudaStream_t st = (cudaStream_t)stream;
+    return dispatch_class(P.n_g, P.n_e, [&](auto C) -> int {
+        using CT = decltype(C);
+        return fp32 ? launch_force<CT, true>(P, pps, st) : launch_force<CT, false>(P, pps, st);
+    });
+}
+
+extern "C" int mm_traj1d_run(const mm_pack *pack, const mm_beams *beams, const double *z0,
+                             const double *v0, int64_t n_particles, double dt, int64_t n_steps,
+                             double z_escape, const mm_batch_opts *opts, double *z_final,
+                             double *v_final, int32_t *n_actual, double *z_traj, double *v_traj,
+                             void *stream)
+{
+    ForceParams P;
+    if (fill_params(pack, beams, opts, P)) return -1;
+    if (!z0 || !v0 || !z_final || !v_final || !n_actual) {
+        mm_set_error("z0, v0, z_final, v_final and n_actual must be non-null");
+        return -1;
+    }
+    if ((z_traj == nullptr) != (v_traj == nullptr)) { mm_set_error("z_traj and v_traj go together"); return -1; }
+    if (n_particles < 0 || n_steps < 1) { mm_set_error("n_particles >= 0 and n_steps >= 1 required"); return -1; }
+    if (n_particles == 0) return 0;
+    P.layout = MM_LAYOUT_POINTS; P.nv = P.nz = 0; P.pps = 1; P.n_points = 0;
+    P.v = P.z = nullptr; P.F = P.R = P.pop = nullptr; P.status = nullptr;
+    TrajParams T;
+    T.dt = dt; T.z_escape = z_escape; T.mass = pack->mass;
+    T.n_particles = n_particles; T.n_steps = n_steps;
+    T.z0 = z0; T.v0 = v0; T.z_final = z_final; T.v_final = v_final;
+    T.z_traj = z_traj; T.v_traj = v_traj; T.n_actual = n_actual;
+    const bool fp32 = opts && opts->precision == MM_PREC_FP32_REFINE;
+    cudaStream_t st = (cudaStream_t)stream;
+    return dispatch_class(P.n_g, P.n_e, [&](auto C) -> int {
+        using CT = decltype(C);
+        return fp32 ? launch_traj<CT, true>(P, T, st) : launch_traj<CT, false>(P, T, st);
+    });
+}

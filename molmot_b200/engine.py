@@ -1,0 +1,235 @@
+"""Device handles and batched calls over the C ABI.
+
+``MoleculePack`` and ``BeamSets`` own the library's immutable device copies
+of a molecule and of parameter sets of beams (the B200 counterpart of
+molmot_cuda's ``CUDAMolData``, molmot_cuda/rate_equations_cuda.py:399-441).
+``force_batch`` and ``traj1d`` launch the CUDA kernels on torch's current
+stream with torch-owned device tensors.  Inputs may be numpy arrays or
+torch tensors; numpy inputs are copied to the device first.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Optional, Sequence
+
+import numpy as np
+import torch
+
+from . import _lib
+from .constants import HBAR_JIT
+
+PRECISIONS = {"fp64": _lib.MM_PREC_FP64, "fp32": _lib.MM_PREC_FP32_REFINE,
+              "fp32_refine": _lib.MM_PREC_FP32_REFINE}
+
+
+def _np(a, dtype):
+    return np.ascontiguousarray(np.asarray(a, dtype=dtype))
+
+
+def _ptr(a: np.ndarray):
+    return ctypes.c_void_p(a.ctypes.data) if a is not None else None
+
+
+def _dptr(t: Optional[torch.Tensor]):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None else None
+
+
+def _device() -> torch.device:
+    if not torch.cuda.is_available():
+        raise RuntimeError("molmot_b200 needs a CUDA device (there is no CPU fallback)")
+    return torch.device("cuda", torch.cuda.current_device())
+
+
+def _to_dev(x, dtype=torch.float64) -> torch.Tensor:
+    dev = _device()
+    if isinstance(x, torch.Tensor):
+        return x.to(device=dev, dtype=dtype).contiguous()
+    return torch.as_tensor(np.ascontiguousarray(x), dtype=dtype).to(dev)
+
+
+def _stream_handle(stream: Optional[torch.cuda.Stream]):
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return ctypes.c_void_p(s.cuda_stream)
+
+
+def molecule_arrays(mol):
+    """Flat host arrays of a MolecularData-like object for the pack."""
+    n_g, n_e = int(mol.n_ground), int(mol.n_excited)
+    out = dict(n_g=n_g, n_e=n_e, E=_np(mol.energies, np.float64),
+               d2=_np(mol.d_squared, np.float64).reshape(-1),
+               zd=_np(mol.zeeman_z_diag, np.float64))
+    if getattr(mol, "zeeman_x", None) is not None and getattr(mol, "tdm", None) is not None:
+        Z = [np.asarray(getattr(mol, f"zeeman_{a}"))[:n_g, :n_g] for a in "xyz"]
+        out["Zre"] = _np(np.stack([z.real for z in Z]), np.float64).reshape(-1)
+        out["Zim"] = _np(np.stack([z.imag for z in Z]), np.float64).reshape(-1)
+        out["Ze"] = _np(np.real(np.diag(np.asarray(mol.zeeman_z)[n_g:, n_g:])), np.float64)
+        tdm = np.asarray(mol.tdm)
+        out["tdm_abs"] = _np(np.abs(tdm[:n_g, n_g:n_g + n_e, :]), np.float64).reshape(-1)
+    return out
+
+
+class MoleculePack:
+    """Device copy of a molecule (energies, |d|^2, Zeeman diagonal, branching
+    ratios; plus ground Zeeman blocks and |tdm| for the 3D model)."""
+
+    def __init__(self, mol):
+        self.mol = mol
+        a = molecule_arrays(mol)
+        self.n_ground, self.n_excited = a["n_g"], a["n_e"]
+        self.Gamma, self.k, self.mass = float(mol.Gamma), float(mol.k), float(mol.mass)
+        self._keep = a
+        d = _lib.MolDesc()
+        d.n_ground, d.n_excited = self.n_ground, self.n_excited
+        d.energies, d.d_squared, d.zeeman_z_diag = _ptr(a["E"]), _ptr(a["d2"]), _ptr(a["zd"])
+        d.Gamma, d.k, d.mass = self.Gamma, self.k, self.mass
+        if "Zre" in a:
+            d.zeeman_ground_re, d.zeeman_ground_im = _ptr(a["Zre"]), _ptr(a["Zim"])
+            d.zeeman_excited_z, d.tdm_abs = _ptr(a["Ze"]), _ptr(a["tdm_abs"])
+        _device()
+        h = ctypes.c_void_p()
+        _lib.check(_lib.load().mm_pack_create(ctypes.byref(d), ctypes.byref(h)), "mm_pack_create")
+        self.handle = h
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and h.value:
+            try:
+                _lib.load().mm_pack_destroy(h)
+            except Exception:
+                pass
+            self.handle = None
+
+
+class BeamSets:
+    """Device copy of ``n_sets`` parameter sets of ``n_beams`` beams.
+
+    kdir, freq, s0: [n_sets, n_beams] float; pol: [n_sets, n_beams] int in
+    {0, 1, 2}; b_gradient: [n_sets] (T/m).  khat [n_sets, n_beams, 3] and
+    radius [n_sets, n_beams] are for the 3D model.
+    """
+
+    def __init__(self, kdir, freq, pol, s0, b_gradient, gamma_eff: float = 1.0,
+                 khat=None, radius=None):
+        kdir = np.atleast_2d(_np(kdir, np.float64))
+        n_sets, n_b = kdir.shape
+        freq = _np(freq, np.float64).reshape(n_sets, n_b)
+        pol = _np(pol, np.int32).reshape(n_sets, n_b)
+        s0 = _np(s0, np.float64).reshape(n_sets, n_b)
+        bg = _np(np.broadcast_to(np.asarray(b_gradient, dtype=np.float64), (n_sets,)), np.float64)
+        self.n_sets, self.n_beams = n_sets, n_b
+        self.gamma_eff = float(gamma_eff)
+        self._keep = [kdir, freq, pol, s0, bg]
+        d = _lib.BeamDesc()
+        d.n_beams = n_b
+        d.kdir, d.freq, d.pol, d.s0, d.b_gradient = (_ptr(kdir), _ptr(freq), _ptr(pol), _ptr(s0),
+                                                     _ptr(bg))
+        d.gamma_eff = self.gamma_eff
+        if khat is not None:
+            kh = _np(khat, np.float64).reshape(n_sets, n_b, 3)
+            rad = _np(radius if radius is not None else np.zeros((n_sets, n_b)), np.float64)
+            rad = rad.reshape(n_sets, n_b)
+            self._keep += [kh, rad]
+            d.khat, d.radius = _ptr(kh), _ptr(rad)
+        _device()
+        h = ctypes.c_void_p()
+        _lib.check(_lib.load().mm_beams_create(ctypes.byref(d), n_sets, ctypes.byref(h)),
+                   "mm_beams_create")
+        self.handle = h
+
+    @classmethod
+    def from_beams(cls, beam_lists: Sequence, b_gradient, gamma_eff: float = 1.0):
+        """From one LaserBeam list or a list of lists (one per set)."""
+        if len(beam_lists) and not isinstance(beam_lists[0], (list, tuple)):
+            beam_lists = [beam_lists]
+        kdir = [[b.kdir_z for b in L] for L in beam_lists]
+        freq = [[b.freq_offset for b in L] for L in beam_lists]
+        pol = [[b.polarization for b in L] for L in beam_lists]
+        s0 = [[b.s0 for b in L] for L in beam_lists]
+        return cls(kdir, freq, pol, s0, b_gradient, gamma_eff)
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and h.value:
+            try:
+                _lib.load().mm_beams_destroy(h)
+            except Exception:
+                pass
+            self.handle = None
+
+
+def _opts(precision, layout, pps=0, nv=0, nz=0, hbar=None, uniform_fallback=False):
+    o = _lib.BatchOpts()
+    o.precision = PRECISIONS[precision] if isinstance(precision, str) else int(precision)
+    o.layout = layout
+    o.points_per_set = int(pps)
+    o.nv, o.nz = int(nv), int(nz)
+    o.hbar = float(hbar) if hbar else HBAR_JIT
+    o.uniform_fallback = 1 if uniform_fallback else 0
+    return o
+
+
+def force_batch(pack: MoleculePack, beams: BeamSets, v, z, *, grid: bool = False,
+                points_per_set: Optional[int] = None, precision="fp64", hbar=None,
+                uniform_fallback: bool = False, want_pop: bool = True, want_R: bool = True,
+                want_status: bool = True, out=None, stream=None):
+    """Steady-state force for a batch of points (one kernel launch).
+
+    grid=True: per set, the outer product of v (nv,) and z (nz,), results
+    shaped [n_sets, nv, nz].  Otherwise v and z are per point and point i
+    belongs to set i // points_per_set; results are flat [n].
+    Returns a dict of device tensors F, R, pop, status.
+    """
+    v = _to_dev(v)
+    z = _to_dev(z)
+    if grid:
+        nv, nz = v.numel(), z.numel()
+        n = beams.n_sets * nv * nz
+        opts = _opts(precision, _lib.MM_LAYOUT_GRID, nv=nv, nz=nz, hbar=hbar,
+                     uniform_fallback=uniform_fallback)
+        shape = (beams.n_sets, nv, nz)
+    else:
+        if v.numel() != z.numel():
+            raise ValueError("points layout needs v and z of the same length")
+        n = v.numel()
+        pps = points_per_set if points_per_set else n
+        opts = _opts(precision, _lib.MM_LAYOUT_POINTS, pps=pps, hbar=hbar,
+                     uniform_fallback=uniform_fallback)
+        shape = (n,)
+    dev = v.device
+    if out is None:
+        out = {"F": torch.empty(shape, dtype=torch.float64, device=dev)}
+        if want_R:
+            out["R"] = torch.empty(shape, dtype=torch.float64, device=dev)
+        if want_pop:
+            out["pop"] = torch.empty(shape + (pack.n_ground,), dtype=torch.float64, device=dev)
+        if want_status:
+            out["status"] = torch.empty(shape, dtype=torch.int32, device=dev)
+    rc = _lib.load().mm_force_batch(pack.handle, beams.handle, _dptr(v), _dptr(z), n,
+                                    ctypes.byref(opts), _dptr(out["F"]), _dptr(out.get("R")),
+                                    _dptr(out.get("pop")), _dptr(out.get("status")),
+                                    _stream_handle(stream))
+    _lib.check(rc, "mm_force_batch")
+    return out
+
+
+def traj1d(pack: MoleculePack, beams: BeamSets, z0, v0, dt: float, n_steps: int, *,
+           z_escape: float = 0.015, save_full: bool = False, precision="fp64", hbar=None,
+           stream=None):
+    """N independent 1D Euler trajectories on the GPU (one launch).
+    Returns device tensors (z_final, v_final, n_actual, z_traj, v_traj)."""
+    z0 = _to_dev(np.atleast_1d(z0) if not isinstance(z0, torch.Tensor) else z0)
+    v0 = _to_dev(np.atleast_1d(v0) if not isinstance(v0, torch.Tensor) else v0)
+    N = z0.numel()
+    dev = z0.device
+    zf = torch.empty(N, dtype=torch.float64, device=dev)
+    vf = torch.empty(N, dtype=torch.float64, device=dev)
+    na = torch.empty(N, dtype=torch.int32, device=dev)
+    zt = torch.empty((N, n_steps), dtype=torch.float64, device=dev) if save_full else None
+    vt = torch.empty((N, n_steps), dtype=torch.float64, device=dev) if save_full else None
+    opts = _opts(precision, _lib.MM_LAYOUT_POINTS, hbar=hbar)
+    rc = _lib.load().mm_traj1d_run(pack.handle, beams.handle, _dptr(z0), _dptr(v0), N, float(dt),
+                                   int(n_steps), float(z_escape), ctypes.byref(opts), _dptr(zf),
+                                   _dptr(vf), _dptr(na), _dptr(zt), _dptr(vt),
+                                   _stream_handle(stream))
+    _lib.check(rc, "mm_traj1d_run")
+    return zf, vf, na, zt, vt

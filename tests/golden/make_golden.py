@@ -1,0 +1,167 @@
+#!/usr/bin/env python3
+"""Generate the golden fixtures in tests/golden/ from the molmot reference.
+
+Run in a container that has the reference checkout (default
+/root/reference, or $MOLMOT_REFERENCE):
+
+    python tests/golden/make_golden.py
+
+It (1) extracts the reference's own golden arrays from
+validation/three_way_results.npz and validation/trajectory_cpu_vs_gpu_results.npz,
+and (2) runs the reference's CPU functions on seeded inputs and saves their
+outputs.  The fixtures are small .npz files; the GPU box, which has no
+reference checkout, reads only these.  Library versions used are recorded
+in each file under the key ``versions``.
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+REF = os.environ.get("MOLMOT_REFERENCE", "/root/reference")
+HERE = os.path.dirname(os.path.abspath(__file__))
+os.environ.setdefault("NUMBA_CACHE_DIR", "/tmp/molmot_numba_cache")
+sys.path.insert(0, REF)
+
+
+def versions():
+    import numba
+    import scipy
+    return np.array(f"numpy {np.__version__}; scipy {scipy.__version__}; numba {numba.__version__}")
+
+
+def beams_to_arrays(beams):
+    return (np.array([b.kdir_z for b in beams]), np.array([b.freq_offset for b in beams]),
+            np.array([b.polarization for b in beams], dtype=np.int32),
+            np.array([b.s0 for b in beams]))
+
+
+def hallas_beams(mol, ratios):
+    """validation/sroh_redmot_three_way.py:67-103 with the given power ratios."""
+    from molmot.constants import c, h
+    from molmot.obe.fields import LaserBeam
+    E = mol.energies
+    n_g, n_e = mol.n_ground, mol.n_excited
+    det = np.array([-10.3, -5.9, -9.2, -29.9]) * 1e6
+    e_last = E[n_g + n_e - 1]
+    freqs = [e_last - E[0] + det[0], e_last - E[0] + det[1],
+             e_last - E[9] + det[2], e_last - E[9] + det[3]]
+    Isat = np.pi * h * c * mol.Gamma / (3.0 * 687e-9 ** 3)
+    r = np.array(ratios, dtype=float)
+    r /= r.sum()
+    sats = (100.0 * 1e-3 * r) * (2.0 / (np.pi * 10e-3 ** 2)) / Isat
+    beams = []
+    for f, q, s in zip(freqs, [2, 0, 2, 0], sats):
+        for d in (+1, -1):
+            qe = q if d > 0 else (2 - q if q != 1 else 1)
+            beams.append(LaserBeam(direction=np.array([0.0, 0.0, float(d)]), freq_offset=f,
+                                   polarization=qe, s0=s))
+    return beams, np.array(freqs), sats
+
+
+def main():
+    from molmot.molecules.sroh import load_sroh_from_julia
+    from molmot.obe.fields import make_dc_mot_beams, make_rf_mot_beams
+    from molmot.obe.rate_equations import solve_rate_equations
+    from molmot.obe.rate_equations_jit import solve_rate_equations_jit
+    from molmot.mot.simulator import DCMOTSimulator, RFMOTSimulator
+    from molmot.mot import force_scan as fs
+    from molmot.propagation.trajectories_jit import simulate_trajectory_jit
+
+    mol = load_sroh_from_julia(os.path.join(REF, "julia_sim"), verbose=False)
+    ver = versions()
+
+    # ---- (1) the reference's own golden arrays: config 1, Hallas ratios ----
+    tw = np.load(os.path.join(REF, "validation", "three_way_results.npz"))
+    beams, freqs, sats = hallas_beams(mol, [0.50, 0.08, 0.15, 0.27])
+    kd, fr, po, s0 = beams_to_arrays(beams)
+    keep = ["z_arr", "v_arr", "Fz_cpu_s", "Fv_cpu_s", "Pz_cpu_s", "k_cpu_s", "beta_cpu_s",
+            "Fz_gpu", "Fv_gpu", "Pz_gpu", "k_gpu", "beta_gpu"]
+    np.savez(os.path.join(HERE, "three_way_golden.npz"),
+             **{k: tw[k] for k in keep}, kdir=kd, freq=fr, pol=po, s0=s0, B_gradient=0.214,
+             F_unit=1.054571817e-34 * mol.k * mol.Gamma / 2.0, versions=ver,
+             source=np.array("validation/three_way_results.npz + sroh_redmot_three_way.py:67-103"))
+
+    # config 1 as BASELINE names it: equal 100 mW split
+    beams_eq, freqs_eq, sats_eq = hallas_beams(mol, [0.25, 0.25, 0.25, 0.25])
+    kd, fr, po, s0 = beams_to_arrays(beams_eq)
+    z = np.linspace(-5e-3, 5e-3, 101)
+    Fz_jit = np.array([solve_rate_equations_jit(mol, beams_eq, 0.0, zi, 0.214)[0] for zi in z])
+    Pz_jit = np.array([solve_rate_equations_jit(mol, beams_eq, 0.0, zi, 0.214)[1] for zi in z])
+    Fz_py = np.array([solve_rate_equations(mol, beams_eq, 0.0, zi, 0.214)[0] for zi in z])
+    sim_like = type("S", (), {})()
+    sim_like.force = lambda v, zz: solve_rate_equations_jit(mol, beams_eq, v, zz, 0.214)
+    k_jit = fs.spring_constant(sim_like)
+    a_jit = fs.damping_coefficient(sim_like)
+    np.savez(os.path.join(HERE, "config1_equal_split.npz"), z=z, Fz_jit=Fz_jit, Pz_jit=Pz_jit,
+             Fz_py=Fz_py, k_jit=k_jit, alpha_jit=a_jit, kdir=kd, freq=fr, pol=po, s0=s0,
+             B_gradient=0.214, sats=sats_eq, versions=ver)
+
+    # ---- (2) seeded random points through the JIT core and the Python path ----
+    rng = np.random.default_rng(20261203)
+    n_sets, n_pts = 24, 16
+    rows = {k: [] for k in ["kdir", "freq", "pol", "s0", "B", "v", "z", "F_jit", "p_jit", "R_jit",
+                            "F_py", "p_py", "R_py"]}
+    for s in range(n_sets):
+        b = make_dc_mot_beams(mol, delta_Gamma=rng.uniform(-3, 0), split_Gamma=rng.uniform(0, 2),
+                              s0=10 ** rng.uniform(-1, 1))
+        kd, fr, po, s0 = beams_to_arrays(b)
+        # per-frequency random detuning/s0 as in the batched-map workload
+        fr = fr + np.repeat(rng.uniform(-40e6, 0, 4), 2)
+        s0 = np.repeat(10 ** rng.uniform(-1, 1, 4), 2)
+        from molmot.obe.fields import LaserBeam
+        b = [LaserBeam(np.array([0.0, 0.0, kd[i]]), fr[i], int(po[i]), s0[i]) for i in range(8)]
+        B = rng.uniform(0.05, 0.4)
+        for _ in range(n_pts):
+            v, zz = rng.uniform(-10, 10), rng.uniform(-1e-2, 1e-2)
+            Fj, pj, Rj = solve_rate_equations_jit(mol, b, v, zz, B)
+            Fp, pp, Rp = solve_rate_equations(mol, b, v, zz, B)
+            for k, val in zip(rows, [kd, fr, po, s0, B, v, zz, Fj, pj, Rj, Fp, pp, Rp]):
+                rows[k].append(val)
+    out = {k: np.array(v) for k, v in rows.items()}
+    np.savez(os.path.join(HERE, "random_points.npz"), n_sets=n_sets, n_pts=n_pts, versions=ver, **out)
+
+    # ---- RF MOT, force_scan API values (DC and RF simulators) ----
+    dc = DCMOTSimulator(mol, delta_Gamma=-0.30, split_Gamma=0.40, s0=1.0, B_gradient=0.16)
+    rf = RFMOTSimulator(mol, delta_Gamma=-1.0, s0=1.0, B_gradient=0.16)
+    zs = np.linspace(-3e-3, 3e-3, 7)
+    vs = np.linspace(-5, 5, 7)
+    F_dc, P_dc, R_dc = fs.force_vs_z(dc, zs)
+    F_rf, P_rf, R_rf = fs.force_vs_z(rf, zs)
+    np.savez(os.path.join(HERE, "force_scan_api.npz"), zs=zs, vs=vs,
+             F_dc_z=F_dc, P_dc_z=P_dc, R_dc_z=R_dc, F_dc_v=fs.force_vs_v(dc, vs),
+             F_rf_z=F_rf, P_rf_z=P_rf, R_rf_z=R_rf, F_rf_v=fs.force_vs_v(rf, vs),
+             k_dc=fs.spring_constant(dc), a_dc=fs.damping_coefficient(dc),
+             k_rf=fs.spring_constant(rf), a_rf=fs.damping_coefficient(rf),
+             vcap_dc=fs.capture_velocity(dc, v_max=6.0, dv=0.5, n_steps=3000),
+             versions=ver)
+    opt = fs.optimize_parameters(mol, {"delta": np.array([-1.0, -0.5, -0.2]),
+                                       "split": np.array([0.2, 0.7])}, 0.16, verbose=False)
+    np.savez(os.path.join(HERE, "optimize_parameters.npz"), delta=opt["delta_scan"],
+             split=opt["split_scan"], K_map=opt["K_map"], beta_map=opt["beta_map"],
+             delta_best=opt["delta_best"], split_best=opt["split_best"], versions=ver)
+
+    # ---- 1D trajectories: the reference's golden endpoints + short JIT runs ----
+    tj = np.load(os.path.join(REF, "validation", "trajectory_cpu_vs_gpu_results.npz"))
+    keep = ["ref_z0", "ref_v0", "ref_zf_py", "ref_vf_py", "ref_zf_jit", "ref_vf_jit",
+            "ref_zf_gpu", "ref_vf_gpu", "batch_z0", "batch_v0", "batch_zf_jit", "batch_vf_jit",
+            "batch_zf_gpu", "batch_vf_gpu", "batch_n_actual", "t_max", "dt"]
+    sim = DCMOTSimulator(mol, delta_Gamma=-0.20, split_Gamma=0.70, s0=1.0, B_gradient=0.16)
+    kd, fr, po, s0 = beams_to_arrays(sim._beams)
+    short = []
+    for z0, v0 in [(3e-3, 0.0), (0.0, -2.0), (2e-3, -1.0), (0.0, -5.0)]:
+        _, za, va = simulate_trajectory_jit(sim, z0, v0, t_max=2e-3, dt=1e-6)
+        short.append((za, va))
+    np.savez(os.path.join(HERE, "trajectory_golden.npz"), **{k: tj[k] for k in keep},
+             kdir=kd, freq=fr, pol=po, s0=s0, B_gradient=0.16,
+             short_z=np.array([s[0] for s in short]), short_v=np.array([s[1] for s in short]),
+             short_t_max=2e-3, versions=ver,
+             source=np.array("validation/trajectory_cpu_vs_gpu_results.npz; short runs: "
+                             "molmot/propagation/trajectories_jit.py simulate_trajectory_jit"))
+    print("golden fixtures written to", HERE)
+
+
+if __name__ == "__main__":
+    main()

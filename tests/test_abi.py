@@ -1,0 +1,77 @@
+"""The C-ABI library: it loads, exports every symbol include/molmot_b200.h
+declares, and rejects bad arguments before touching the GPU (no compute
+calls here, so this runs without a GPU)."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+HEADER = os.path.join(ROOT, "include", "molmot_b200.h")
+
+
+def declared_symbols():
+    src = open(HEADER).read()
+    return sorted(set(re.findall(r"MM_API\s+(?:const\s+)?\w+\s*\*?\s*(mm_\w+)\s*\(", src)))
+
+
+def test_header_declares_entry_points():
+    syms = declared_symbols()
+    for s in ["mm_pack_create", "mm_beams_create", "mm_force_batch", "mm_traj1d_run",
+              "mm_last_error"]:
+        assert s in syms
+
+
+def test_library_exports_every_declared_symbol():
+    from molmot_b200 import _lib
+    L = _lib.load()
+    for s in declared_symbols():
+        assert hasattr(L, s), s
+        assert s in _lib.SIGNATURES, f"{s} has no ctypes signature"
+
+
+def test_version_and_error_strings():
+    from molmot_b200 import _lib
+    L = _lib.load()
+    assert b"sm_100a" in L.mm_version()
+    assert isinstance(L.mm_last_error(), bytes)
+
+
+def test_pack_create_rejects_bad_sizes():
+    from molmot_b200 import _lib
+    L = _lib.load()
+    d = _lib.MolDesc()
+    E = np.zeros(2)
+    d.n_ground, d.n_excited = 0, 1
+    d.energies = d.d_squared = d.zeeman_z_diag = ctypes.c_void_p(E.ctypes.data)
+    d.Gamma, d.k, d.mass = 1.0, 1.0, 1.0
+    h = ctypes.c_void_p()
+    assert L.mm_pack_create(ctypes.byref(d), ctypes.byref(h)) < 0
+    assert b"out of range" in L.mm_last_error()
+    assert not h.value
+
+
+def test_beams_create_rejects_bad_polarisation():
+    from molmot_b200 import _lib
+    L = _lib.load()
+    kd = np.ones(2)
+    pol = np.array([0, 5], dtype=np.int32)
+    d = _lib.BeamDesc()
+    d.n_beams = 2
+    d.kdir = d.freq = d.s0 = d.b_gradient = ctypes.c_void_p(kd.ctypes.data)
+    d.pol = ctypes.c_void_p(pol.ctypes.data)
+    h = ctypes.c_void_p()
+    assert L.mm_beams_create(ctypes.byref(d), 1, ctypes.byref(h)) < 0
+    assert b"polarization" in L.mm_last_error()
+
+
+def test_force_batch_rejects_null_handles():
+    from molmot_b200 import _lib
+    L = _lib.load()
+    o = _lib.BatchOpts()
+    rc = L.mm_force_batch(None, None, None, None, 1, ctypes.byref(o), None, None, None, None, None)
+    assert rc < 0
+    assert b"null" in L.mm_last_error()
