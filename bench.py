@@ -145,6 +145,28 @@ def cpu_baseline(mol, n_sets_sample=8):
                       f"prange over points, os.cpu_count()={os.cpu_count()}"}
 
 
+def oracle_check(mol, pack, bs, v_d, z_d, kdir, freq, pol, s0, B, sets=(0, 1, 2047, 4095)):
+    """Both GPU forms against the CPU oracle on a few whole sets (the checker;
+    part of the cpu_baseline leg, rank 0 only)."""
+    import torch
+    from molmot_b200.engine import force_batch
+    from oracle import rate_eq as orc
+    v_h = v_d.cpu().numpy()
+    z_h = z_d.cpu().numpy()
+    sets = [s for s in sets if s < kdir.shape[0]]
+    Fo = orc.force_batch(mol, kdir[sets], freq[sets], pol[sets], s0[sets], B[sets], v_h, z_h,
+                         grid=True, want_pop=False)[0].reshape(len(sets), -1)
+    res = {}
+    for prec in ("fp64", "fp32"):
+        o = force_batch(pack, bs, v_d, z_d, grid=True, precision=prec, want_pop=False,
+                        want_R=False, want_status=False)
+        F = o["F"].cpu().numpy().reshape(kdir.shape[0], -1)[sets]
+        errs = np.max(np.abs(F - Fo), axis=1) / np.max(np.abs(Fo), axis=1)
+        res[prec] = {"max": float(errs.max()), "sets": [int(s) for s in sets]}
+    torch.cuda.synchronize()
+    return res
+
+
 def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -251,8 +273,17 @@ def main():
     clocks = ClockSampler(local)
     clocks.start()
     ms32 = timed("fp32", args.steps, args.warmup)
+    F32 = out["F"].clone()
     ms64 = timed("fp64", args.steps, args.warmup)
     clk = clocks.stop()
+    # per-set accuracy of the FP32 form against the plain FP64 form (every set)
+    scale = out["F"].abs().amax(dim=(1, 2))
+    err_sets = ((F32 - out["F"]).abs().amax(dim=(1, 2)) / scale).cpu().numpy()
+    del F32
+    accuracy = {"fp32_vs_fp64_per_set": {"max": float(err_sets.max()),
+                                         "median": float(np.median(err_sets)),
+                                         "p99": float(np.quantile(err_sets, 0.99)),
+                                         "sets": int(err_sets.size)}}
 
     # end to end through the public API with host buffers
     pinned_F = torch.empty((n_sets, NV, NZ), dtype=torch.float64, pin_memory=True)
@@ -297,6 +328,7 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(mol)
+        accuracy["vs_oracle"] = oracle_check(mol, pack, bs, v_d, z_d, kdir, freq, pol, s0, B)
 
     if rank == 0:
         total = n_pts * world
@@ -323,6 +355,7 @@ def main():
             "e2e": {"value": total / (ms_e2e * 1e-3), "unit": "force evals/s",
                     "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                     "ms_per_step": ms_e2e},
+            "accuracy": accuracy,
             "gpu_launches": args.steps * 2,
             "clocks": clk,
         }

@@ -14,8 +14,8 @@ namespace {
 
 constexpr int kThreads = 128;
 
-template <int NGMAX, int NEMAX, int G, bool FP32>
-__global__ void __launch_bounds__(kThreads)
+template <int NGMAX, int NEMAX, int G, bool FP32, bool EXACT>
+__global__ void __launch_bounds__(kThreads, 3)
 force_kernel(ForceParams P)
 {
     using GS = GroupShape<NGMAX, NEMAX, G>;
@@ -55,7 +55,8 @@ force_kernel(ForceParams P)
                 z = P.z[set_first + ipc];
             }
             double xs[GS::CPL];
-            const PointOut o = solve_point<NGMAX, NEMAX, G, FP32>(P, S, fd, Ese, t, gbase, v, z, Bg, xs);
+            const PointOut o = solve_point<NGMAX, NEMAX, G, FP32, EXACT>(P, S, fd, Ese, t, gbase, v, z,
+                                                                          Bg, xs);
             if (valid) {
                 const long long gi = set_first + ip;
                 if (t == 0) {
@@ -85,8 +86,8 @@ struct TrajParams {
 
 // Fused 1D Euler trajectories (molmot/propagation/trajectories_jit.py:18-58):
 // v_j = v_{j-1} + F(v_{j-1}, z_{j-1})/m dt; z_j = z_{j-1} + v_j dt; stop when |z| > z_escape.
-template <int NGMAX, int NEMAX, int G, bool FP32>
-__global__ void __launch_bounds__(kThreads)
+template <int NGMAX, int NEMAX, int G, bool FP32, bool EXACT>
+__global__ void __launch_bounds__(kThreads, 3)
 traj1d_kernel(ForceParams P, TrajParams T)
 {
     using GS = GroupShape<NGMAX, NEMAX, G>;
@@ -111,7 +112,8 @@ traj1d_kernel(ForceParams P, TrajParams T)
     for (long long j = 1; j < T.n_steps; j++) {
         if (__all_sync(0xffffffffu, done)) break;
         double xs[GS::CPL];
-        const PointOut o = solve_point<NGMAX, NEMAX, G, FP32>(P, S, fd, Ese, t, gbase, v, z, Bg, xs);
+        const PointOut o = solve_point<NGMAX, NEMAX, G, FP32, EXACT>(P, S, fd, Ese, t, gbase, v, z, Bg,
+                                                                      xs);
         if (!done) {
             const double a = o.F / T.mass;
             v = v + a * T.dt;
@@ -135,10 +137,11 @@ traj1d_kernel(ForceParams P, TrajParams T)
     }
 }
 
-// Size classes: (NGMAX, NEMAX, G).
-template <int NGMAX, int NEMAX, int G>
+// Size classes: (NGMAX, NEMAX, G, EXACT).
+template <int NGMAX, int NEMAX, int G, bool EXACT>
 struct Class {
     static constexpr int ng = NGMAX, ne = NEMAX, g = G;
+    static constexpr bool exact = EXACT;
 };
 
 template <class C, bool FP32>
@@ -152,7 +155,7 @@ size_t smem_bytes(const ForceParams &P)
 template <class C, bool FP32>
 int launch_force(const ForceParams &P, long long pts_per_set, cudaStream_t st)
 {
-    auto kern = force_kernel<C::ng, C::ne, C::g, FP32>;
+    auto kern = force_kernel<C::ng, C::ne, C::g, FP32, C::exact>;
     const size_t sb = smem_bytes<C, FP32>(P);
     if (sb > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb);
@@ -181,7 +184,7 @@ int launch_force(const ForceParams &P, long long pts_per_set, cudaStream_t st)
 template <class C, bool FP32>
 int launch_traj(const ForceParams &P, const TrajParams &T, cudaStream_t st)
 {
-    auto kern = traj1d_kernel<C::ng, C::ne, C::g, FP32>;
+    auto kern = traj1d_kernel<C::ng, C::ne, C::g, FP32, C::exact>;
     const size_t sb = smem_bytes<C, FP32>(P);
     if (sb > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb);
@@ -197,7 +200,8 @@ int launch_traj(const ForceParams &P, const TrajParams &T, cudaStream_t st)
 template <class F>
 int dispatch_class(int n_g, int n_e, F &&f)
 {
-    if (n_g <= 12 && n_e <= 4) return f(Class<12, 4, 4>{});
+    if (n_g == 12 && n_e == 4) return f(Class<12, 4, 4, true>{});   // SrOH
+    if (n_g <= 12 && n_e <= 4) return f(Class<12, 4, 4, false>{});
     mm_set_error("molecule size n_ground=%d n_excited=%d exceeds the register-resident 1D "
                  "kernel class (n_ground <= 12, n_excited <= 4)", n_g, n_e);
     return -1;
