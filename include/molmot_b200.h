@@ -121,6 +121,33 @@ MM_API int mm_force_batch(const mm_pack *pack, const mm_beams *beams, const doub
                    const double *z, int64_t n_points, const mm_batch_opts *opts,
                    double *F, double *R, double *pop, int32_t *status, void *stream);
 
+/* Options of mm_traj_run. */
+typedef struct {
+    int32_t ndim;      /* 1: along z; 3: per-axis model of trajectories.py:78-156        */
+    int32_t n_avg;     /* 1: beam set 0; 2: average of sets 0 and 1 (RF MOT phases)      */
+    int64_t n_steps;   /* samples per trajectory, the initial one included               */
+    double dt;         /* s                                                              */
+    double r_escape;   /* m: |z| (ndim 1) or |r| (ndim 3) beyond which a particle stops  */
+    int64_t i_eq;      /* first step whose v^2 enters vsq_sum (with vsq_sum non-NULL)    */
+    int32_t precision; /* MM_PREC_*                                                      */
+    int32_t reserved;
+    double hbar;       /* J s; <= 0 selects 1.0545718e-34                                */
+} mm_traj_opts;
+
+/*
+ * Independent trajectories, one launch for all steps.  ndim = 1 replaces
+ * traj_kernel / simulate_trajectories_cuda (molmot_cuda/trajectories_cuda.py:44-280,
+ * 305-426) and _trajectory_1d_jit (molmot/propagation/trajectories_jit.py:18-58);
+ * ndim = 3 replaces simulate_trajectories_3d (molmot/propagation/trajectories.py:78-156);
+ * with vsq_sum / n_samp it also accumulates the sums of monte_carlo_temperature
+ * (molmot/propagation/trajectories.py:159-229).  Arrays are [N][ndim]
+ * (r_traj / v_traj: [N][n_steps][ndim], nullable; vsq_sum / n_samp: [N], nullable).
+ */
+MM_API int mm_traj_run(const mm_pack *pack, const mm_beams *beams, const mm_traj_opts *opts,
+                       const double *r0, const double *v0, int64_t n_particles,
+                       double *r_final, double *v_final, int32_t *n_actual, double *r_traj,
+                       double *v_traj, double *vsq_sum, double *n_samp, void *stream);
+
 /*
  * N independent 1D trajectories with symplectic Euler, one beam set (set 0).
  * Replaces traj_kernel / simulate_trajectories_cuda

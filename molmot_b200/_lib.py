@@ -49,6 +49,13 @@ class BatchOpts(ctypes.Structure):
                 ("uniform_fallback", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
 
+class TrajOpts(ctypes.Structure):
+    _fields_ = [("ndim", ctypes.c_int32), ("n_avg", ctypes.c_int32), ("n_steps", ctypes.c_int64),
+                ("dt", ctypes.c_double), ("r_escape", ctypes.c_double), ("i_eq", ctypes.c_int64),
+                ("precision", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("hbar", ctypes.c_double)]
+
+
 #: every symbol include/molmot_b200.h declares, with (restype, argtypes)
 SIGNATURES = {
     "mm_last_error": (ctypes.c_char_p, []),
@@ -62,6 +69,8 @@ SIGNATURES = {
     "mm_traj1d_run": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_int64, ctypes.c_double,
                                      ctypes.c_int64, ctypes.c_double, ctypes.POINTER(BatchOpts),
                                      _vp, _vp, _vp, _vp, _vp, _vp]),
+    "mm_traj_run": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(TrajOpts), _vp, _vp, ctypes.c_int64,
+                                   _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "mm_peak_probe": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int64, _dp, _dp, _vp]),
 }
 

@@ -79,13 +79,31 @@ force_kernel(ForceParams P)
 struct TrajParams {
     double dt, z_escape, mass;
     long long n_particles, n_steps;
-    const double *z0, *v0;
-    double *z_final, *v_final, *z_traj, *v_traj;
-    int32_t *n_actual;
+    int ndim;         // 1: along z;  3: per-axis model (x, y, z)
+    int n_avg;        // parameter sets averaged per force evaluation (RF MOT: 2 phases)
+    long long i_eq;   // first step whose v^2 enters vsq_sum (temperature); < 0: off
+    const double *z0, *v0;          // [N][ndim]
+    double *z_final, *v_final;      // [N][ndim]
+    double *z_traj, *v_traj;        // [N][n_steps][ndim] or null
+    int32_t *n_actual;              // [N]
+    double *vsq_sum, *n_samp;       // [N] or null
 };
 
-// Fused 1D Euler trajectories (molmot/propagation/trajectories_jit.py:18-58):
-// v_j = v_{j-1} + F(v_{j-1}, z_{j-1})/m dt; z_j = z_{j-1} + v_j dt; stop when |z| > z_escape.
+// Fused trajectories, one particle per group, all steps in one launch.
+//  ndim = 1: symplectic Euler along z (molmot/propagation/trajectories_jit.py:18-58,
+//            molmot_cuda/trajectories_cuda.py:44-280):
+//            v_j = v_{j-1} + F(v_{j-1}, z_{j-1})/m dt; z_j = z_{j-1} + v_j dt;
+//            stop when |z| > z_escape (n_actual = j, the rest of the row repeats).
+//  ndim = 3: the per-axis model of molmot/propagation/trajectories.py:78-156:
+//            F_z = F(v_z, z), F_x = F(v_x, -x/2), F_y = F(v_y, -y/2), the same Euler
+//            update per axis, stop when |r| > z_escape.  F(v, -x/2) is computed as
+//            F at coordinate x with gradient -B'/2 (bit-identical product).
+//  n_avg = 2: force = 0.5 (F_set0 + F_set1), the RF MOT time average
+//            (molmot/mot/simulator.py:49-90; the sets carry +B' and -B').
+//  vsq_sum / n_samp: sums of v^2 over steps j >= i_eq that did not escape
+//            (molmot/propagation/trajectories.py:159-229, monte_carlo_temperature).
+// The integrator uses explicit round-to-nearest operations so it matches the
+// reference's uncontracted arithmetic.
 template <int NGMAX, int NEMAX, int G, bool FP32, bool EXACT>
 __global__ void __launch_bounds__(kThreads, 3)
 traj1d_kernel(ForceParams P, TrajParams T)
@@ -99,41 +117,74 @@ traj1d_kernel(ForceParams P, TrajParams T)
     const int group = threadIdx.x / G;
     double *scr = (double *)(sm + Ly.scratch) + (size_t)group * Ly.scratch_per_group;
     double *fd = scr, *Ese = scr + P.n_b;
-    SetView S;
-    build_set_tables<G, GS::CPL, FP32>(P, 0, sm, Ly, S);
-    const double Bg = P.bgrad[0];
-
+    SetView S[2];
+    double Bg[2];
+    for (int a = 0; a < T.n_avg; a++) {
+        build_set_tables<G, GS::CPL, FP32>(P, a, sm + a * Ly.total, Ly, S[a]);
+        Bg[a] = P.bgrad[a];
+    }
+    const int nd = T.ndim;
     const long long ip = (long long)blockIdx.x * ngroups + group;
     const bool valid = ip < T.n_particles;
-    double z = valid ? T.z0[ip] : 0.0, v = valid ? T.v0[ip] : 0.0;
+    double x[3] = {0.0, 0.0, 0.0}, u[3] = {0.0, 0.0, 0.0};
+    for (int d = 0; d < nd; d++) {
+        x[d] = valid ? T.z0[ip * nd + d] : 0.0;
+        u[d] = valid ? T.v0[ip * nd + d] : 0.0;
+    }
     long long na = T.n_steps;
     bool done = !valid;
-    if (valid && T.z_traj && t == 0) { T.z_traj[ip * T.n_steps] = z; T.v_traj[ip * T.n_steps] = v; }
+    double vsq = 0.0, nsamp = 0.0;
+    const long long row = ip * T.n_steps * nd;
+    if (valid && T.z_traj && t == 0)
+        for (int d = 0; d < nd; d++) { T.z_traj[row + d] = x[d]; T.v_traj[row + d] = u[d]; }
     for (long long j = 1; j < T.n_steps; j++) {
         if (__all_sync(0xffffffffu, done)) break;
-        double xs[GS::CPL];
-        const PointOut o = solve_point<NGMAX, NEMAX, G, FP32, EXACT>(P, S, fd, Ese, t, gbase, v, z, Bg,
-                                                                      xs);
+        double acc[3];
+        for (int d = 0; d < nd; d++) {
+            // axis multipliers of B' in the per-axis model: x, y see -B'/2, z sees B'
+            const double mult = (nd == 3 && d < 2) ? -0.5 : 1.0;
+            double F = 0.0;
+            for (int a = 0; a < T.n_avg; a++) {
+                double xs[GS::CPL];
+                const PointOut o = solve_point<NGMAX, NEMAX, G, FP32, EXACT>(
+                    P, S[a], fd, Ese, t, gbase, u[d], x[d], Bg[a] * mult, xs);
+                F = (a == 0) ? o.F : __dadd_rn(F, o.F);
+            }
+            if (T.n_avg == 2) F = 0.5 * F;
+            acc[d] = __ddiv_rn(F, T.mass);
+        }
         if (!done) {
-            const double a = o.F / T.mass;
-            v = v + a * T.dt;
-            z = z + v * T.dt;
-            if (T.z_traj && t == 0) { T.z_traj[ip * T.n_steps + j] = z; T.v_traj[ip * T.n_steps + j] = v; }
-            if (fabs(z) > T.z_escape) {
+            double r2 = 0.0;
+            for (int d = 0; d < nd; d++) {
+                u[d] = __dadd_rn(u[d], __dmul_rn(acc[d], T.dt));
+                x[d] = __dadd_rn(x[d], __dmul_rn(u[d], T.dt));
+                r2 = fma(x[d], x[d], r2);
+            }
+            if (T.z_traj && t == 0)
+                for (int d = 0; d < nd; d++) {
+                    T.z_traj[row + j * nd + d] = x[d];
+                    T.v_traj[row + j * nd + d] = u[d];
+                }
+            const bool esc = (nd == 1) ? (fabs(x[0]) > T.z_escape) : (sqrt(r2) > T.z_escape);
+            if (esc) {
                 na = j;
                 done = true;
                 if (T.z_traj && t == 0)
-                    for (long long s = j + 1; s < T.n_steps; s++) {
-                        T.z_traj[ip * T.n_steps + s] = z;
-                        T.v_traj[ip * T.n_steps + s] = v;
-                    }
+                    for (long long s = j + 1; s < T.n_steps; s++)
+                        for (int d = 0; d < nd; d++) {
+                            T.z_traj[row + s * nd + d] = x[d];
+                            T.v_traj[row + s * nd + d] = u[d];
+                        }
+            } else if (T.i_eq >= 0 && j >= T.i_eq) {
+                for (int d = 0; d < nd; d++) vsq = __dadd_rn(vsq, __dmul_rn(u[d], u[d]));
+                nsamp += 1.0;
             }
         }
     }
     if (valid && t == 0) {
-        T.z_final[ip] = z;
-        T.v_final[ip] = v;
+        for (int d = 0; d < nd; d++) { T.z_final[ip * nd + d] = x[d]; T.v_final[ip * nd + d] = u[d]; }
         T.n_actual[ip] = (int32_t)na;
+        if (T.vsq_sum) { T.vsq_sum[ip] = vsq; T.n_samp[ip] = nsamp; }
     }
 }
 
@@ -185,7 +236,7 @@ template <class C, bool FP32>
 int launch_traj(const ForceParams &P, const TrajParams &T, cudaStream_t st)
 {
     auto kern = traj1d_kernel<C::ng, C::ne, C::g, FP32, C::exact>;
-    const size_t sb = smem_bytes<C, FP32>(P);
+    const size_t sb = smem_bytes<C, FP32>(P) * T.n_avg;
     if (sb > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb);
         if (mm_cuda_check(e, "cudaFuncSetAttribute")) return -3;
@@ -273,32 +324,66 @@ extern "C" int mm_force_batch(const mm_pack *pack, const mm_beams *beams, const 
     });
 }
 
+extern "C" int mm_traj_run(const mm_pack *pack, const mm_beams *beams, const mm_traj_opts *topt,
+                           const double *r0, const double *v0, int64_t n_particles,
+                           double *r_final, double *v_final, int32_t *n_actual, double *r_traj,
+                           double *v_traj, double *vsq_sum, double *n_samp, void *stream)
+{
+    if (!topt) { mm_set_error("trajectory options are required"); return -1; }
+    mm_batch_opts bo = {};
+    bo.precision = topt->precision;
+    bo.hbar = topt->hbar;
+    ForceParams P;
+    if (fill_params(pack, beams, &bo, P)) return -1;
+    if (!r0 || !v0 || !r_final || !v_final || !n_actual) {
+        mm_set_error("r0, v0, r_final, v_final and n_actual must be non-null");
+        return -1;
+    }
+    if ((r_traj == nullptr) != (v_traj == nullptr)) { mm_set_error("r_traj and v_traj go together"); return -1; }
+    if ((vsq_sum == nullptr) != (n_samp == nullptr)) { mm_set_error("vsq_sum and n_samp go together"); return -1; }
+    if (n_particles < 0 || topt->n_steps < 1) { mm_set_error("n_particles >= 0 and n_steps >= 1 required"); return -1; }
+    if (topt->ndim != 1 && topt->ndim != 3) { mm_set_error("ndim must be 1 or 3"); return -1; }
+    if (topt->n_avg < 1 || topt->n_avg > 2 || topt->n_avg > beams->n_sets) {
+        mm_set_error("n_avg=%d must be 1 or 2 and <= n_sets=%d", topt->n_avg, beams->n_sets);
+        return -1;
+    }
+    if (topt->precision != MM_PREC_FP64 && topt->precision != MM_PREC_FP32_REFINE) {
+        mm_set_error("unknown precision %d", topt->precision);
+        return -1;
+    }
+    if (n_particles == 0) return 0;
+    P.layout = MM_LAYOUT_POINTS; P.nv = P.nz = 0; P.pps = 1; P.n_points = 0;
+    P.v = P.z = nullptr; P.F = P.R = P.pop = nullptr; P.status = nullptr;
+    TrajParams T;
+    T.dt = topt->dt; T.z_escape = topt->r_escape; T.mass = pack->mass;
+    T.n_particles = n_particles; T.n_steps = topt->n_steps;
+    T.ndim = topt->ndim; T.n_avg = topt->n_avg; T.i_eq = vsq_sum ? topt->i_eq : -1;
+    T.z0 = r0; T.v0 = v0; T.z_final = r_final; T.v_final = v_final;
+    T.z_traj = r_traj; T.v_traj = v_traj; T.n_actual = n_actual;
+    T.vsq_sum = vsq_sum; T.n_samp = n_samp;
+    const bool fp32 = topt->precision == MM_PREC_FP32_REFINE;
+    cudaStream_t st = (cudaStream_t)stream;
+    return dispatch_class(P.n_g, P.n_e, [&](auto C) -> int {
+        using CT = decltype(C);
+        return fp32 ? launch_traj<CT, true>(P, T, st) : launch_traj<CT, false>(P, T, st);
+    });
+}
+
 extern "C" int mm_traj1d_run(const mm_pack *pack, const mm_beams *beams, const double *z0,
                              const double *v0, int64_t n_particles, double dt, int64_t n_steps,
                              double z_escape, const mm_batch_opts *opts, double *z_final,
                              double *v_final, int32_t *n_actual, double *z_traj, double *v_traj,
                              void *stream)
 {
-    ForceParams P;
-    if (fill_params(pack, beams, opts, P)) return -1;
-    if (!z0 || !v0 || !z_final || !v_final || !n_actual) {
-        mm_set_error("z0, v0, z_final, v_final and n_actual must be non-null");
-        return -1;
-    }
-    if ((z_traj == nullptr) != (v_traj == nullptr)) { mm_set_error("z_traj and v_traj go together"); return -1; }
-    if (n_particles < 0 || n_steps < 1) { mm_set_error("n_particles >= 0 and n_steps >= 1 required"); return -1; }
-    if (n_particles == 0) return 0;
-    P.layout = MM_LAYOUT_POINTS; P.nv = P.nz = 0; P.pps = 1; P.n_points = 0;
-    P.v = P.z = nullptr; P.F = P.R = P.pop = nullptr; P.status = nullptr;
-    TrajParams T;
-    T.dt = dt; T.z_escape = z_escape; T.mass = pack->mass;
-    T.n_particles = n_particles; T.n_steps = n_steps;
-    T.z0 = z0; T.v0 = v0; T.z_final = z_final; T.v_final = v_final;
-    T.z_traj = z_traj; T.v_traj = v_traj; T.n_actual = n_actual;
-    const bool fp32 = opts && opts->precision == MM_PREC_FP32_REFINE;
-    cudaStream_t st = (cudaStream_t)stream;
-    return dispatch_class(P.n_g, P.n_e, [&](auto C) -> int {
-        using CT = decltype(C);
-        return fp32 ? launch_traj<CT, true>(P, T, st) : launch_traj<CT, false>(P, T, st);
-    });
+    mm_traj_opts T = {};
+    T.ndim = 1;
+    T.n_avg = 1;
+    T.n_steps = n_steps;
+    T.dt = dt;
+    T.r_escape = z_escape;
+    T.i_eq = -1;
+    T.precision = opts ? opts->precision : MM_PREC_FP64;
+    T.hbar = opts ? opts->hbar : 0.0;
+    return mm_traj_run(pack, beams, &T, z0, v0, n_particles, z_final, v_final, n_actual, z_traj,
+                       v_traj, nullptr, nullptr, stream);
 }

@@ -212,24 +212,70 @@ def force_batch(pack: MoleculePack, beams: BeamSets, v, z, *, grid: bool = False
     return out
 
 
+def traj(pack: MoleculePack, beams: BeamSets, r0, v0, dt: float, n_steps: int, *, ndim: int = 1,
+         n_avg: int = 1, r_escape: float = 0.015, save_full: bool = False, i_eq: Optional[int] = None,
+         precision="fp64", hbar=None, stream=None):
+    """Independent trajectories on the GPU, all steps in one launch.
+
+    ndim = 1: Euler along z; r0, v0 are (N,).  ndim = 3: the per-axis model;
+    r0, v0 are (N, 3).  n_avg = 2 averages beam sets 0 and 1 (RF MOT).
+    i_eq: also return per-particle sums of v^2 and sample counts over steps
+    j >= i_eq (monte_carlo_temperature).  Returns a dict of device tensors
+    r_final, v_final, n_actual and optionally r_traj, v_traj, vsq_sum, n_samp.
+    """
+    r0 = _to_dev(r0).reshape(-1, ndim)
+    v0 = _to_dev(v0).reshape(-1, ndim)
+    N = r0.shape[0]
+    dev = r0.device
+    out = {"r_final": torch.empty((N, ndim), dtype=torch.float64, device=dev),
+           "v_final": torch.empty((N, ndim), dtype=torch.float64, device=dev),
+           "n_actual": torch.empty(N, dtype=torch.int32, device=dev)}
+    if save_full:
+        out["r_traj"] = torch.empty((N, n_steps, ndim), dtype=torch.float64, device=dev)
+        out["v_traj"] = torch.empty((N, n_steps, ndim), dtype=torch.float64, device=dev)
+    if i_eq is not None:
+        out["vsq_sum"] = torch.empty(N, dtype=torch.float64, device=dev)
+        out["n_samp"] = torch.empty(N, dtype=torch.float64, device=dev)
+    o = _lib.TrajOpts()
+    o.ndim, o.n_avg, o.n_steps = int(ndim), int(n_avg), int(n_steps)
+    o.dt, o.r_escape = float(dt), float(r_escape)
+    o.i_eq = int(i_eq) if i_eq is not None else -1
+    o.precision = PRECISIONS[precision] if isinstance(precision, str) else int(precision)
+    o.hbar = float(hbar) if hbar else HBAR_JIT
+    rc = _lib.load().mm_traj_run(pack.handle, beams.handle, ctypes.byref(o), _dptr(r0), _dptr(v0), N,
+                                 _dptr(out["r_final"]), _dptr(out["v_final"]),
+                                 _dptr(out["n_actual"]), _dptr(out.get("r_traj")),
+                                 _dptr(out.get("v_traj")), _dptr(out.get("vsq_sum")),
+                                 _dptr(out.get("n_samp")), _stream_handle(stream))
+    _lib.check(rc, "mm_traj_run")
+    return out
+
+
 def traj1d(pack: MoleculePack, beams: BeamSets, z0, v0, dt: float, n_steps: int, *,
            z_escape: float = 0.015, save_full: bool = False, precision="fp64", hbar=None,
            stream=None):
-    """N independent 1D Euler trajectories on the GPU (one launch).
+    """N independent 1D Euler trajectories (beam set 0).
     Returns device tensors (z_final, v_final, n_actual, z_traj, v_traj)."""
-    z0 = _to_dev(np.atleast_1d(z0) if not isinstance(z0, torch.Tensor) else z0)
-    v0 = _to_dev(np.atleast_1d(v0) if not isinstance(v0, torch.Tensor) else v0)
-    N = z0.numel()
-    dev = z0.device
-    zf = torch.empty(N, dtype=torch.float64, device=dev)
-    vf = torch.empty(N, dtype=torch.float64, device=dev)
-    na = torch.empty(N, dtype=torch.int32, device=dev)
-    zt = torch.empty((N, n_steps), dtype=torch.float64, device=dev) if save_full else None
-    vt = torch.empty((N, n_steps), dtype=torch.float64, device=dev) if save_full else None
-    opts = _opts(precision, _lib.MM_LAYOUT_POINTS, hbar=hbar)
-    rc = _lib.load().mm_traj1d_run(pack.handle, beams.handle, _dptr(z0), _dptr(v0), N, float(dt),
-                                   int(n_steps), float(z_escape), ctypes.byref(opts), _dptr(zf),
-                                   _dptr(vf), _dptr(na), _dptr(zt), _dptr(vt),
-                                   _stream_handle(stream))
-    _lib.check(rc, "mm_traj1d_run")
-    return zf, vf, na, zt, vt
+    o = traj(pack, beams, np.atleast_1d(z0) if not isinstance(z0, torch.Tensor) else z0,
+             np.atleast_1d(v0) if not isinstance(v0, torch.Tensor) else v0, dt, n_steps, ndim=1,
+             r_escape=z_escape, save_full=save_full, precision=precision, hbar=hbar, stream=stream)
+    zt = o["r_traj"][..., 0] if save_full else None
+    vt = o["v_traj"][..., 0] if save_full else None
+    return o["r_final"][:, 0], o["v_final"][:, 0], o["n_actual"], zt, vt
+
+
+_PACKS = {}
+
+
+def pack_for(mol) -> MoleculePack:
+    """Cached MoleculePack of a molecule object (rebuilt when its arrays change)."""
+    key = id(mol)
+    a = molecule_arrays(mol)
+    fp = hash((a["E"].tobytes(), a["d2"].tobytes(), a["zd"].tobytes(), float(mol.Gamma),
+               float(mol.k), float(mol.mass)))
+    hit = _PACKS.get(key)
+    if hit is not None and hit[0] is mol and hit[1] == fp:
+        return hit[2]
+    p = MoleculePack(mol)
+    _PACKS[key] = (mol, fp, p)
+    return p

@@ -160,6 +160,21 @@ def main():
              short_t_max=2e-3, versions=ver,
              source=np.array("validation/trajectory_cpu_vs_gpu_results.npz; short runs: "
                              "molmot/propagation/trajectories_jit.py simulate_trajectory_jit"))
+    # ---- per-axis 3D trajectories, RF trajectory, Monte-Carlo temperature ----
+    from molmot.propagation.trajectories import (simulate_trajectories_3d, simulate_trajectory,
+                                                 monte_carlo_temperature)
+    dc2 = DCMOTSimulator(mol, delta_Gamma=-0.20, split_Gamma=0.70, s0=1.0, B_gradient=0.16)
+    r0s = [np.array([1e-3, -0.5e-3, 2e-3]), np.array([0.0, 2e-3, -1e-3])]
+    v0s = [np.array([0.5, -0.3, 1.0]), np.array([-1.0, 0.2, 0.0])]
+    tr3 = simulate_trajectories_3d(dc2, r0s, v0s, t_max=6e-4, dt=1e-6)
+    rf2 = RFMOTSimulator(mol, delta_Gamma=-1.0, s0=1.0, B_gradient=0.16)
+    _, zrf, vrf = simulate_trajectory(rf2, 2e-3, -1.0, t_max=8e-4, dt=1e-6)
+    T_mc = monte_carlo_temperature(dc2, n_particles=6, t_max=1.5e-3, dt=1e-6,
+                                   t_equilibrium=0.5e-3)
+    np.savez(os.path.join(HERE, "trajectory_api_golden.npz"),
+             r0=np.array(r0s), v0=np.array(v0s), r3=np.array([t[1] for t in tr3]),
+             v3=np.array([t[2] for t in tr3]), t_max3=6e-4, z_rf=zrf, v_rf=vrf, t_max_rf=8e-4,
+             T_mc=T_mc, mc_n=6, mc_t_max=1.5e-3, mc_t_eq=0.5e-3, versions=ver)
     print("golden fixtures written to", HERE)
 
 

@@ -1,0 +1,75 @@
+"""Host-side logic that needs no GPU: inputs, samplers, simulator adapters."""
+import numpy as np
+import pytest
+
+from conftest import golden
+
+
+def test_sroh_loader_matches_golden_beams(mol):
+    from molmot_b200.fields import make_dc_mot_beams
+    g = golden("trajectory_golden.npz")
+    b = make_dc_mot_beams(mol, delta_Gamma=-0.20, split_Gamma=0.70, s0=1.0)
+    assert np.array_equal([x.freq_offset for x in b], g["freq"])
+    assert np.array_equal([x.polarization for x in b], g["pol"])
+    assert np.array_equal([x.kdir_z for x in b], g["kdir"])
+
+
+def test_molecule_derived_fields(mol):
+    assert mol.d_squared.shape == (12, 4, 3)
+    assert int((mol.d_squared > 1e-15).sum()) == 39
+    assert mol.omega_J32 > mol.omega_J12  # J=1/2 lies ~55 MHz above J=3/2
+    from molmot_b200.flops import active_triples, flops_per_point
+    from molmot_b200.fields import make_dc_mot_beams
+    pols = [b.polarization for b in make_dc_mot_beams(mol)]
+    A = active_triples(mol.d_squared, pols)
+    assert A == 96
+    assert abs(flops_per_point(12, 4, 8, A)[0] - 4822) < 1
+
+
+def test_constants():
+    from molmot_b200 import constants as C
+    from molmot_b200.molecules import K_WAVE, MASS_KG
+    assert abs(C.v_recoil(K_WAVE, MASS_KG) - 5.53e-3) < 0.02e-3
+    assert C.HBAR_JIT != C.hbar
+
+
+def test_samplers_moments():
+    from molmot_b200 import trajectories as tr
+    rng = np.random.default_rng(42)
+    v = tr.sample_maxwell_boltzmann(5e-3, 1.74356601993e-25, 10000, rng)
+    sigma = np.sqrt(1.380649e-23 * 5e-3 / 1.74356601993e-25)
+    assert abs(v.std() / sigma - 1) < 0.1 and abs(sigma - 0.629) < 0.01
+    r = tr.sample_gaussian_position(1e-3, 10000, rng)
+    assert abs(r.std() / 1e-3 - 1) < 0.1
+    d = np.array([tr.sample_direction(rng) for _ in range(2000)])
+    assert np.allclose(np.linalg.norm(d, axis=1), 1.0)
+    assert np.all(np.abs(d.mean(0)) < 0.1)
+    u = tr.sample_uniform_sphere(2e-3, 500, rng)
+    assert np.all(np.linalg.norm(u, axis=1) <= 2e-3)
+
+
+def test_as_gpu_simulator_rejects_unknown():
+    from molmot_b200.simulator import as_gpu_simulator
+    with pytest.raises(TypeError):
+        as_gpu_simulator(object())
+
+
+def test_reference_simulator_objects_adapt(mol):
+    """The reference's DC/RF simulator classes map onto GPU simulators
+    (attribute-compatible), checked without launching anything."""
+    from molmot_b200.simulator import as_gpu_simulator, BeamListSimulator, RFMOTSimulator
+
+    class RefDC:
+        pass
+    s = RefDC()
+    s.mol_data, s._beams, s.B_gradient, s.Gamma_eff_factor = mol, [], 0.16, 1.0
+    assert isinstance(as_gpu_simulator(s), BeamListSimulator)
+
+    class RefRF:
+        pass
+    r = RefRF()
+    r.mol_data, r.delta_Gamma, r.s0, r.B_gradient, r.Gamma_eff_factor = mol, -1.0, 1.0, 0.16, 1.0
+    g = as_gpu_simulator(r)
+    assert isinstance(g, RFMOTSimulator)
+    (b0, B0), (b1, B1) = g.param_sets()
+    assert B0 == -B1 and [x.polarization for x in b0] != [x.polarization for x in b1]
