@@ -162,6 +162,41 @@ MM_API int mm_traj1d_run(const mm_pack *pack, const mm_beams *beams, const doubl
                   void *stream);
 
 /*
+ * 3D steady-state force at points (r[i], v[i]) (arrays [n][3]); point i uses
+ * beam set i / points_per_set.  Replaces rate_eq_force_3d
+ * (molmot/mot/simulator_3d.py:168-365) and rate_eq_force_3d_batch
+ * (molmot_cuda/simulator_3d_cuda.py:666-754; that kernel's Jacobi eigensolver
+ * is replaced by a correct one).  Needs a pack with the 3D fields and beam
+ * sets with khat.  hbar <= 0 selects CODATA 1.054571817e-34 (the 3D
+ * reference path's value).  Outputs: F[n][3], R[n] (nullable),
+ * pop[n][n_ground] (nullable), status[n] (nullable).
+ */
+MM_API int mm_force3d_batch(const mm_pack *pack, const mm_beams *beams, const double *r,
+                            const double *v, int64_t n_points, int64_t points_per_set, double hbar,
+                            double *F, double *R, double *pop, int32_t *status, void *stream);
+
+/*
+ * 3D leapfrog ensemble, one launch for all steps (beam set 0).  Replaces
+ * MOTSimulator3D.simulate_trajectory_3d / simulate_ensemble_3d
+ * (molmot/mot/simulator_3d.py:443-532) and simulate_ensemble_3d_cuda
+ * (molmot_cuda/simulator_3d_cuda.py:890-973).  step0 = 0: v0 is the initial
+ * velocity and the first half kick is applied; step0 > 0 resumes a run:
+ * r0 / v0 are r_out / vh_out of the previous call (checkpoint).  kicks != 0
+ * adds photon-recoil kicks: N ~ Poisson(R dt) events per step, 2N isotropic
+ * kicks of hbar k / m, random numbers from Philox4x32-10 keyed by seed with
+ * counter (particle, step, draw, 0) -- reproducible across checkpoints.
+ * Outputs [N][3]: r_out, vh_out (half-step velocity), v_out (synchronised,
+ * nullable); n_actual[N]; r_traj / v_traj [N][n_steps][3] (nullable);
+ * ke[N] = m |v|^2 / 2 at the end (nullable); n_events[N] (nullable).
+ */
+MM_API int mm_traj3d_run(const mm_pack *pack, const mm_beams *beams, const double *r0,
+                         const double *v0, int64_t n_particles, int64_t step0, int64_t n_steps,
+                         double dt, double r_escape, int32_t kicks, uint64_t seed, double hbar,
+                         double *r_out, double *vh_out, double *v_out, int32_t *n_actual,
+                         double *r_traj, double *v_traj, double *ke, int32_t *n_events,
+                         void *stream);
+
+/*
  * FMA-throughput probe (measurement aid; no counterpart in the reference).
  * which = 0: FP64, 1: FP32.  Runs a register-only FMA loop on every SM and
  * writes its duration (ms) and FLOP count (2 per FMA); synchronises `stream`.

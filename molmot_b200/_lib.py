@@ -71,6 +71,12 @@ SIGNATURES = {
                                      _vp, _vp, _vp, _vp, _vp, _vp]),
     "mm_traj_run": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(TrajOpts), _vp, _vp, ctypes.c_int64,
                                    _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "mm_force3d_batch": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_int64, ctypes.c_int64,
+                                        ctypes.c_double, _vp, _vp, _vp, _vp, _vp]),
+    "mm_traj3d_run": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_int64, ctypes.c_int64,
+                                     ctypes.c_int64, ctypes.c_double, ctypes.c_double,
+                                     ctypes.c_int32, ctypes.c_uint64, ctypes.c_double,
+                                     _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "mm_peak_probe": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int64, _dp, _dp, _vp]),
 }
 

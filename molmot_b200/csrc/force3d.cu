@@ -1,0 +1,702 @@
+// force3d.cu -- 3D rate-equation force (quadrupole field, ground Zeeman
+// eigenbasis, per-beam polarisation weights, Gaussian beams) and the fused
+// 3D leapfrog ensemble with photon-recoil kicks; C-ABI entry points
+// mm_force3d_batch and mm_traj3d_run.
+//
+// Reference: molmot/mot/simulator_3d.py:168-365 (rate_eq_force_3d, the CPU
+// path with numpy eigh -- the only correct 3D reference; the reference's own
+// GPU kernel, molmot_cuda/simulator_3d_cuda.py:53-562, converges to wrong
+// eigenvalues) and :443-504 (simulate_trajectory_3d, leapfrog).
+//
+// One point per group of 16 lanes (two per warp).  Per point:
+//  1. B = B'(-x/2, -y/2, z) 1e4 G;  H = B.Z (ground block), Hermitianised.
+//  2. Cyclic Jacobi eigen-decomposition of the complex Hermitian H in shared
+//     memory, round-robin (circle) ordering: the n/2 disjoint rotations of a
+//     round are computed by n/2 lanes and applied by all 16 lanes.  Sweeps
+//     continue until the off-diagonal norm is below 1e-30 of the diagonal
+//     norm (warp-uniform).  Eigenvalues are sorted ascending with their
+//     vectors, as numpy.linalg.eigh returns them; Es_g[i] = E_g[i] + lambda_i.
+//  3. |U^H |tdm||^2 per (eigenstate, e, q); branching ratios.
+//  4. Lane g accumulates, over beams and excited states, the unsaturated rates,
+//     s_total[g] and the per-state force vector in one pass (the saturation
+//     factor 1/(1+s_total[g]) is common to all of a state's terms).
+//  5. Population matrix, Gaussian elimination with partial pivoting (lane k
+//     holds column k), clamp, normalise (uniform populations if all clamp).
+//  6. F = hbar k sum_b khat_b rate_b p, R = sum rate p.
+#include <stdio.h>
+#include <algorithm>
+#include "rate_core.cuh"
+
+namespace {
+
+constexpr int kG3 = 16;        // lanes per point
+constexpr int kThreads3 = 128; // 8 points per CTA
+constexpr int NGM = 12;        // max ground states of the 3D kernel (SrOH-sized)
+constexpr int NEM = 4;         // max excited states
+constexpr int NBM = 32;        // max beams
+constexpr int LDH = NGM + 1;   // padded row length of the matrices in shared memory
+
+struct Force3Params {
+    int n_g, n_e, n_b, n_sets;
+    double Gamma, k, hbar, geff, mass;
+    const double *E, *Zre, *Zim, *Ze, *tdm;  // pack arrays
+    const double *khat, *freq, *s0, *radius, *bgrad;
+    const int32_t *pol;
+    long long n_points, pps;
+    const double *r, *v;                       // [n][3]
+    double *F, *R, *pop;                       // [n][3], [n], [n][n_g]
+    int32_t *status;
+    int uniform_fb;
+};
+
+struct Traj3Params {
+    double dt, r_escape;
+    long long n_particles, n_steps, step0;
+    int kicks;
+    unsigned long long seed;
+    const double *r0, *v0;          // [N][3]; v0 is the half-step velocity when step0 > 0
+    double *r_out, *vh_out, *v_out; // [N][3]: position, half-step velocity, synchronised velocity
+    int32_t *n_actual;              // [N] steps completed (escape step or n_steps)
+    double *r_traj, *v_traj;        // [N][n_steps][3] or null
+    double *ke_sum;                 // [N] or null: final 0.5 m |v|^2
+    int32_t *n_events;              // [N] or null: scattering events drawn
+};
+
+// Per-CTA constants (molecule + one beam set) and per-group work arrays.
+struct Smem3 {
+    double Zre[3][NGM * NGM], Zim[3][NGM * NGM];
+    double tdm[NGM * NEM * 3];
+    double E[NGM + NEM], Ze[NEM];
+    double khat[NBM][3], freq[NBM], s0[NBM], radius[NBM];
+    int pol[NBM];
+    struct Group {
+        double Hre[NGM * LDH], Him[NGM * LDH];
+        double Vre[NGM * LDH], Vim[NGM * LDH];
+        double rot[NGM / 2][3];      // c, Re s, Im s
+        double lam[NGM];
+        int perm[NGM];
+        double dsq[NGM * NEM * 3];
+        double BR[NEM * NGM];
+        double Esg[NGM], Ese[NEM];
+        double bm[NBM][5];           // doppler, s_eff, w0, w1, w2
+    } grp[kThreads3 / kG3];
+};
+
+__device__ __forceinline__ double gsum16(double x)
+{
+#pragma unroll
+    for (int o = 8; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    return x;
+}
+
+// Pair (p, q) of round r, slot i of the circle schedule on n (even) players.
+__device__ __forceinline__ void rr_pair(int n, int r, int i, int &p, int &q)
+{
+    auto pos = [&](int j) { return j == 0 ? 0 : ((r + j - 1) % (n - 1)) + 1; };
+    p = pos(i);
+    q = pos(n - 1 - i);
+}
+
+__device__ void load_consts3(const Force3Params &P, int set, Smem3 &S)
+{
+    const int n_g = P.n_g, n_e = P.n_e, n_b = P.n_b, tid = threadIdx.x, nt = blockDim.x;
+    for (int i = tid; i < 3 * n_g * n_g; i += nt) {
+        const int a = i / (n_g * n_g), rc = i % (n_g * n_g);
+        S.Zre[a][rc] = P.Zre[i];
+        S.Zim[a][rc] = P.Zim[i];
+    }
+    for (int i = tid; i < n_g * n_e * 3; i += nt) S.tdm[i] = P.tdm[i];
+    for (int i = tid; i < n_g + n_e; i += nt) S.E[i] = P.E[i];
+    for (int i = tid; i < n_e; i += nt) S.Ze[i] = P.Ze[i];
+    const size_t o = (size_t)set * n_b;
+    for (int b = tid; b < n_b; b += nt) {
+        for (int c = 0; c < 3; c++) S.khat[b][c] = P.khat[(o + b) * 3 + c];
+        S.freq[b] = P.freq[o + b];
+        S.s0[b] = P.s0[o + b];
+        S.radius[b] = P.radius ? P.radius[o + b] : 0.0;
+        S.pol[b] = P.pol[o + b];
+    }
+}
+
+struct Out3 {
+    double F[3], R;
+    int status;
+};
+
+// The 3D force at (r, v) for the group of 16 lanes (lane t, base gbase).
+// pl receives the population of ground state t (t < n_g).
+__device__ Out3 force3d_point(const Force3Params &P, Smem3 &S, Smem3::Group &W, int t, int gbase,
+                              const double r[3], const double v[3], double Bg, double &pl)
+{
+    constexpr unsigned FULL = 0xffffffffu;
+    const int n_g = P.n_g, n_e = P.n_e, n_b = P.n_b;
+    const double G = P.Gamma;
+    int stat = 0;
+
+    // 1. field and Hermitian Zeeman matrix
+    const double B0 = ((-Bg * r[0]) / 2.0) * 1e4;
+    const double B1 = ((-Bg * r[1]) / 2.0) * 1e4;
+    const double B2 = (Bg * r[2]) * 1e4;
+    const double Bm = sqrt(B0 * B0 + B1 * B1 + B2 * B2);
+    // only the z component of B_hat enters the polarisation weights (cos theta)
+    const double bh2 = (Bm > 1e-10) ? B2 / Bm : 1.0;
+    __syncwarp();
+    for (int idx = t; idx < n_g * n_g; idx += kG3) {
+        const int i = idx / n_g, j = idx % n_g;
+        const int ij = i * n_g + j, ji = j * n_g + i;
+        const double hr = (B0 * S.Zre[0][ij] + B1 * S.Zre[1][ij]) + B2 * S.Zre[2][ij];
+        const double hi = (B0 * S.Zim[0][ij] + B1 * S.Zim[1][ij]) + B2 * S.Zim[2][ij];
+        const double gr = (B0 * S.Zre[0][ji] + B1 * S.Zre[1][ji]) + B2 * S.Zre[2][ji];
+        const double gi = (B0 * S.Zim[0][ji] + B1 * S.Zim[1][ji]) + B2 * S.Zim[2][ji];
+        W.Hre[i * LDH + j] = 0.5 * (hr + gr);   // 0.5 (H + H^H)
+        W.Him[i * LDH + j] = 0.5 * (hi - gi);
+        W.Vre[i * LDH + j] = (i == j) ? 1.0 : 0.0;
+        W.Vim[i * LDH + j] = 0.0;
+    }
+    __syncwarp();
+
+    // 2. cyclic Jacobi, circle ordering
+    const int n = (n_g + 1) & ~1;  // even number of players (one dummy when n_g is odd)
+    const int npair = n / 2;
+    for (int sweep = 0; sweep < 30; sweep++) {
+        // convergence: off-diagonal vs diagonal squared norms
+        double off = 0.0, dia = 0.0;
+        for (int idx = t; idx < n_g * n_g; idx += kG3) {
+            const int i = idx / n_g, j = idx % n_g;
+            const double a2 = W.Hre[i * LDH + j] * W.Hre[i * LDH + j] + W.Him[i * LDH + j] * W.Him[i * LDH + j];
+            if (i == j) dia += a2; else off += a2;
+        }
+        off = gsum16(off);
+        dia = gsum16(dia);
+        const bool more = off > 1e-30 * dia && off > 1e-300;
+        if (!__any_sync(FULL, more)) break;
+        for (int rnd = 0; rnd < n - 1; rnd++) {
+            if (t < npair) {
+                int p, q;
+                rr_pair(n, rnd, t, p, q);
+                double c = 1.0, sr = 0.0, si = 0.0;
+                if (p < n_g && q < n_g) {
+                    const double a = W.Hre[p * LDH + p], b = W.Hre[q * LDH + q];
+                    const double xr = W.Hre[p * LDH + q], xi = W.Him[p * LDH + q];
+                    const double rho = sqrt(xr * xr + xi * xi);
+                    if (rho > 1e-300 && rho > 1e-18 * (fabs(a) + fabs(b))) {
+                        const double tau = (b - a) / (2.0 * rho);
+                        const double tt = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
+                        c = 1.0 / sqrt(1.0 + tt * tt);
+                        const double s = tt * c;
+                        sr = s * xr / rho;   // s e^{i phi}
+                        si = s * xi / rho;
+                    }
+                }
+                W.rot[t][0] = c; W.rot[t][1] = sr; W.rot[t][2] = si;
+            }
+            __syncwarp();
+            // columns p, q of H and V:  X' = X J,  J = [[c, s],[-conj(s), c]]
+            for (int w = t; w < 2 * npair * n_g; w += kG3) {
+                const int mat = w / (npair * n_g), rem = w % (npair * n_g);
+                const int pi = rem / n_g, row = rem % n_g;
+                int p, q;
+                rr_pair(n, rnd, pi, p, q);
+                if (p >= n_g || q >= n_g) continue;
+                double *Xr = mat ? W.Vre : W.Hre, *Xi = mat ? W.Vim : W.Him;
+                const double c = W.rot[pi][0], sr = W.rot[pi][1], si = W.rot[pi][2];
+                const double apr = Xr[row * LDH + p], api = Xi[row * LDH + p];
+                const double aqr = Xr[row * LDH + q], aqi = Xi[row * LDH + q];
+                // a_p' = a_p c - a_q conj(s);  a_q' = a_p s + a_q c
+                Xr[row * LDH + p] = apr * c - (aqr * sr + aqi * si);
+                Xi[row * LDH + p] = api * c - (aqi * sr - aqr * si);
+                Xr[row * LDH + q] = (apr * sr - api * si) + aqr * c;
+                Xi[row * LDH + q] = (apr * si + api * sr) + aqi * c;
+            }
+            __syncwarp();
+            // rows p, q of H:  H' = J^H H
+            for (int w = t; w < npair * n_g; w += kG3) {
+                const int pi = w / n_g, col = w % n_g;
+                int p, q;
+                rr_pair(n, rnd, pi, p, q);
+                if (p >= n_g || q >= n_g) continue;
+                const double c = W.rot[pi][0], sr = W.rot[pi][1], si = W.rot[pi][2];
+                const double apr = W.Hre[p * LDH + col], api = W.Him[p * LDH + col];
+                const double aqr = W.Hre[q * LDH + col], aqi = W.Him[q * LDH + col];
+                // a_p' = c a_p - s a_q;  a_q' = conj(s) a_p + c a_q
+                W.Hre[p * LDH + col] = c * apr - (sr * aqr - si * aqi);
+                W.Him[p * LDH + col] = c * api - (sr * aqi + si * aqr);
+                W.Hre[q * LDH + col] = (sr * apr + si * api) + c * aqr;
+                W.Him[q * LDH + col] = (sr * api - si * apr) + c * aqi;
+            }
+            __syncwarp();
+            if (t < npair) {  // exact zero of the rotated pair, real diagonal
+                int p, q;
+                rr_pair(n, rnd, t, p, q);
+                if (p < n_g && q < n_g && (W.rot[t][1] != 0.0 || W.rot[t][2] != 0.0)) {
+                    W.Hre[p * LDH + q] = 0.0; W.Him[p * LDH + q] = 0.0;
+                    W.Hre[q * LDH + p] = 0.0; W.Him[q * LDH + p] = 0.0;
+                    W.Him[p * LDH + p] = 0.0; W.Him[q * LDH + q] = 0.0;
+                }
+            }
+            __syncwarp();
+        }
+    }
+    // ascending order (ties by index), as eigh returns the spectrum
+    if (t < n_g) {
+        const double lt = W.Hre[t * LDH + t];
+        int rank = 0;
+        for (int j = 0; j < n_g; j++) {
+            const double lj = W.Hre[j * LDH + j];
+            rank += (lj < lt || (lj == lt && j < t)) ? 1 : 0;
+        }
+        W.perm[rank] = t;
+        W.lam[rank] = lt;
+    }
+    __syncwarp();
+    // 3. energies and |U^H d|^2 in the eigenbasis (lane a = sorted eigenstate)
+    if (t < n_g) W.Esg[t] = S.E[t] + W.lam[t] * G / (2 * MM_PI);
+    if (t < n_e)  // exact order of simulator_3d.py:241-243
+        W.Ese[t] = __dadd_rn(S.E[n_g + t], __ddiv_rn(__dmul_rn(__dmul_rn(B2, S.Ze[t]), G), MM_TWO_PI));
+    double rowsum[NEM];
+#pragma unroll
+    for (int e = 0; e < NEM; e++) rowsum[e] = 0.0;
+    if (t < n_g) {
+        const int col = W.perm[t];
+        for (int e = 0; e < n_e; e++) {
+            for (int q = 0; q < 3; q++) {
+                double ar = 0.0, ai = 0.0;
+                for (int g = 0; g < n_g; g++) {
+                    const double d = S.tdm[(g * n_e + e) * 3 + q];
+                    ar += W.Vre[g * LDH + col] * d;   // conj(U[g, col]) d
+                    ai -= W.Vim[g * LDH + col] * d;
+                }
+                const double d2 = ar * ar + ai * ai;
+                W.dsq[(t * n_e + e) * 3 + q] = d2;
+                rowsum[e] += d2;
+            }
+        }
+    }
+    // branching ratios BR[e][a] = sum_q dsq[a,e,q] / sum_{a,q} dsq[a,e,q]
+#pragma unroll
+    for (int e = 0; e < NEM; e++) {
+        const double tot = gsum16(rowsum[e]);
+        if (t < n_g && e < n_e) W.BR[e * n_g + t] = tot > 1e-30 ? rowsum[e] / tot : 0.0;
+    }
+    // per-beam doppler, Gaussian-weighted s0 and local polarisation weights
+    const double ct = fmin(fmax(bh2, -1.0), 1.0);
+    const double st = sin(acos(ct));
+    const double wd = ((1 + ct) / 2) * ((1 + ct) / 2), wo = ((1 - ct) / 2) * ((1 - ct) / 2);
+    const double wm = (st / sqrt(2.0)) * (st / sqrt(2.0)), wc = ct * ct;
+    for (int b = t; b < n_b; b += kG3) {
+        // doppler -k (khat . v) / 2pi in the reference's uncontracted order
+        const double kv = __dadd_rn(__dadd_rn(__dmul_rn(S.khat[b][0], v[0]), __dmul_rn(S.khat[b][1], v[1])),
+                                    __dmul_rn(S.khat[b][2], v[2]));
+        W.bm[b][0] = __ddiv_rn(__dmul_rn(-P.k, kv), MM_TWO_PI);
+        double gf = 1.0;
+        if (S.radius[b] > 0.0) {
+            const double rp = r[0] * S.khat[b][0] + r[1] * S.khat[b][1] + r[2] * S.khat[b][2];
+            const double rps = fmax((r[0] * r[0] + r[1] * r[1] + r[2] * r[2]) - rp * rp, 0.0);
+            gf = exp(-2.0 * rps / (S.radius[b] * S.radius[b]));
+        }
+        W.bm[b][1] = S.s0[b] * gf;
+        // column q of |d^1(theta)|^2 (rows m_local = -1, 0, +1), normalised
+        const int q = S.pol[b];
+        double w0, w1, w2;
+        if (q == 0) { w0 = wd; w1 = wm; w2 = wo; }
+        else if (q == 1) { w0 = wm; w1 = wc; w2 = wm; }
+        else { w0 = wo; w1 = wm; w2 = wd; }
+        const double ws = w0 + w1 + w2;
+        if (ws > 1e-15) { w0 /= ws; w1 /= ws; w2 /= ws; }
+        W.bm[b][2] = w0; W.bm[b][3] = w1; W.bm[b][4] = w2;
+    }
+    __syncwarp();
+
+    // 4. rates of ground eigenstate g = t, one pass over beams and excited states
+    const double gh = G / 2.0, gh2 = gh * gh;
+    double Racc[NEM], Fv[3] = {0.0, 0.0, 0.0}, sg = 0.0;
+#pragma unroll
+    for (int e = 0; e < NEM; e++) Racc[e] = 0.0;
+    if (t < n_g) {
+        const double Eg = W.Esg[t];
+        for (int b = 0; b < n_b; b++) {
+            const double fd = __dadd_rn(S.freq[b], W.bm[b][0]);
+            const double se = W.bm[b][1];
+            double Qb = 0.0;
+#pragma unroll
+            for (int e = 0; e < NEM; e++) {
+                if (e < n_e) {
+                    const double om = __dsub_rn(W.Ese[e], Eg);
+                    const double de = __dmul_rn(__dsub_rn(fd, om), MM_TWO_PI);
+                    const double L = gh2 * mm_rcp(fma(de, de, gh2));
+                    double ws = 0.0;
+#pragma unroll
+                    for (int q = 0; q < 3; q++) {
+                        const double d2 = W.dsq[(t * n_e + e) * 3 + q];
+                        if (d2 >= 1e-15) ws = fma(W.bm[b][2 + q], d2, ws);
+                    }
+                    const double rb = ws * L * se;
+                    Racc[e] += rb;
+                    Qb += rb;
+                }
+            }
+            sg += Qb;
+            Fv[0] = fma(S.khat[b][0], Qb, Fv[0]);
+            Fv[1] = fma(S.khat[b][1], Qb, Fv[1]);
+            Fv[2] = fma(S.khat[b][2], Qb, Fv[2]);
+        }
+    }
+    const double cg = gh * P.geff * mm_rcp(1.0 + sg);  // rate = cg * unsaturated sum
+    double Rk = 0.0;
+#pragma unroll
+    for (int e = 0; e < NEM; e++) { Racc[e] *= cg; Rk += Racc[e]; }
+
+    // 5. population matrix (lane k owns column k), elimination, back substitution
+    double A[NGM], bv[NGM];
+#pragma unroll
+    for (int i = 0; i < NGM; i++) {
+        double a = 0.0;
+        if (t < n_g && i < n_g) {
+            a = (i == t) ? -Rk : 0.0;
+#pragma unroll
+            for (int e = 0; e < NEM; e++)
+                if (e < n_e) a = fma(Racc[e], W.BR[e * n_g + i], a);
+            if (i == n_g - 1) a = 1.0;
+        } else if (i == t) {
+            a = 1.0;  // identity padding
+        }
+        A[i] = a;
+        bv[i] = (i == n_g - 1) ? 1.0 : 0.0;
+    }
+    double invd = 0.0;
+#pragma unroll
+    for (int col = 0; col < NGM; col++) {
+        if (col < n_g) {
+            int prow = col;
+            if (t == col) {
+                double mx = fabs(A[col]);
+#pragma unroll
+                for (int rr = col + 1; rr < NGM; rr++)
+                    if (rr < n_g && fabs(A[rr]) > mx) { mx = fabs(A[rr]); prow = rr; }
+            }
+            prow = __shfl_sync(FULL, prow, gbase + col);
+            if (__any_sync(FULL, prow != col)) {
+#pragma unroll
+                for (int rr = col + 1; rr < NGM; rr++)
+                    if (rr == prow) {
+                        double x = A[col]; A[col] = A[rr]; A[rr] = x;
+                        x = bv[col]; bv[col] = bv[rr]; bv[rr] = x;
+                    }
+            }
+            double inv_e = 0.0;
+            if (t == col) {
+                const double ap = fabs(A[col]);
+                const double y = mm_rcp(ap >= 1e-30 ? A[col] : 1.0);
+                inv_e = ap < 1e-30 ? 0.0 : y;
+                invd = ap > 1e-30 ? y : 0.0;
+                if (ap < 1e-30) stat |= MM_ST_PIVOT;
+            }
+#pragma unroll
+            for (int rr = col + 1; rr < NGM; rr++) {
+                if (rr < n_g) {
+                    double f = (t == col) ? A[rr] * inv_e : 0.0;
+                    f = __shfl_sync(FULL, f, gbase + col);
+                    if (t > col) A[rr] = fma(-f, A[col], A[rr]);
+                    bv[rr] = fma(-f, bv[col], bv[rr]);
+                }
+            }
+        }
+    }
+    double x = 0.0;
+#pragma unroll
+    for (int i = NGM - 1; i >= 0; i--) {
+        if (i < n_g) {
+            double part = (t > i && t < n_g) ? A[i] * x : 0.0;
+            part = gsum16(part);
+            if (t == i) x = (bv[i] - part) * invd;
+        }
+    }
+    if (t >= n_g || x < 0.0) x = 0.0;
+    const double tot = gsum16(x);
+    if (tot > 0.0) x *= mm_rcp(tot);
+    else {
+        stat |= MM_ST_ZERO_POP;
+        if (P.uniform_fb) x = (t < n_g) ? 1.0 / n_g : 0.0;
+    }
+    pl = x;
+    // 6. force and scattering rate
+    const double hk = P.hbar * P.k;
+    Out3 o;
+    const double wgt = (t < n_g) ? x * cg : 0.0;
+    o.F[0] = hk * gsum16(wgt * Fv[0]);
+    o.F[1] = hk * gsum16(wgt * Fv[1]);
+    o.F[2] = hk * gsum16(wgt * Fv[2]);
+    o.R = gsum16((t < n_g) ? x * Rk : 0.0);
+    if (!isfinite(o.F[0]) || !isfinite(o.F[1]) || !isfinite(o.F[2])) stat |= MM_ST_NONFINITE;
+    o.status = stat;
+    for (int off = 8; off > 0; off >>= 1) o.status |= __shfl_xor_sync(FULL, o.status, off);
+    return o;
+}
+
+__global__ void __launch_bounds__(kThreads3)
+force3d_kernel(Force3Params P)
+{
+    extern __shared__ __align__(16) unsigned char smraw[];
+    Smem3 &S = *reinterpret_cast<Smem3 *>(smraw);
+    const int lane = threadIdx.x & 31, t = lane % kG3, gbase = lane - t;
+    const int group = threadIdx.x / kG3, ngroups = kThreads3 / kG3;
+    for (int set = blockIdx.y; set < P.n_sets; set += gridDim.y) {
+        const long long first = (long long)set * P.pps;
+        long long count = P.pps;
+        if (first + count > P.n_points) count = P.n_points - first;
+        if (count <= 0) continue;
+        __syncthreads();
+        load_consts3(P, set, S);
+        __syncthreads();
+        const double Bg = P.bgrad[set];
+        for (long long base = (long long)blockIdx.x * ngroups; base < count;
+             base += (long long)gridDim.x * ngroups) {
+            const long long ip = base + group;
+            const bool valid = ip < count;
+            const long long gi = first + (valid ? ip : 0);
+            double r[3], v[3], pl;
+            for (int c = 0; c < 3; c++) { r[c] = P.r[gi * 3 + c]; v[c] = P.v[gi * 3 + c]; }
+            const Out3 o = force3d_point(P, S, S.grp[group], t, gbase, r, v, Bg, pl);
+            if (valid) {
+                if (t == 0) {
+                    for (int c = 0; c < 3; c++) P.F[gi * 3 + c] = o.F[c];
+                    if (P.R) P.R[gi] = o.R;
+                    if (P.status) P.status[gi] = o.status;
+                }
+                if (P.pop && t < P.n_g) P.pop[gi * P.n_g + t] = pl;
+            }
+        }
+    }
+}
+
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11): 10 rounds of
+// (hi(M0 c0) ^ c1 ^ k0, lo(M1 c2), hi(M1 c2) ^ c3 ^ k1, lo(M0 c0)) with Weyl key bumps.
+__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k)
+{
+    const unsigned M0 = 0xD2511F53u, M1 = 0xCD9E8D57u, W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+#pragma unroll
+    for (int i = 0; i < 10; i++) {
+        const unsigned hi0 = __umulhi(M0, c.x), lo0 = M0 * c.x;
+        const unsigned hi1 = __umulhi(M1, c.z), lo1 = M1 * c.z;
+        c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
+        k.x += W0;
+        k.y += W1;
+    }
+    return c;
+}
+
+__device__ __forceinline__ double u01(unsigned x) { return ((double)x + 0.5) * 2.3283064365386963e-10; }
+
+// Recoil kick of one step (the oracle's recoil_kick): N ~ Poisson(lam) by
+// sequential inversion, then 2N isotropic unit vectors times v_rec.
+__device__ int recoil_kick(unsigned long long seed, unsigned particle, unsigned step, double lam,
+                           double v_rec, double kick[3])
+{
+    const uint2 key = make_uint2((unsigned)(seed & 0xffffffffu), (unsigned)(seed >> 32));
+    const uint4 u0 = philox4x32_10(make_uint4(particle, step, 0u, 0u), key);
+    const double u = u01(u0.x);
+    double p = exp(-lam), F = p;
+    int n = 0;
+    while (u > F && n < 256) {
+        n++;
+        p *= lam / n;
+        F += p;
+    }
+    kick[0] = kick[1] = kick[2] = 0.0;
+    for (int i = 0; i < 2 * n; i += 2) {
+        const uint4 w = philox4x32_10(make_uint4(particle, step, 1u + (unsigned)(i / 2), 0u), key);
+        const double a[2] = {u01(w.x), u01(w.z)}, b[2] = {u01(w.y), u01(w.w)};
+        for (int h = 0; h < 2; h++) {
+            const double cz = 2.0 * a[h] - 1.0, phi = 2.0 * MM_PI * b[h];
+            const double sp = sqrt(fmax(0.0, 1.0 - cz * cz));
+            kick[0] += v_rec * (sp * cos(phi));
+            kick[1] += v_rec * (sp * sin(phi));
+            kick[2] += v_rec * cz;
+        }
+    }
+    return n;
+}
+
+// Leapfrog ensemble (simulator_3d.py:443-504):
+//   v_1/2 = v_0 + (0.5 dt) F(r_0, v_0)/m;  r_j = r_{j-1} + dt v_half;
+//   escape when |r_j| > r_escape (position and half-step velocity freeze);
+//   F = F(r_j, v_half); v_new = v_half + dt F/m (+ recoil kick); v_j = (v_half + v_new)/2.
+__global__ void __launch_bounds__(kThreads3)
+traj3d_kernel(Force3Params P, Traj3Params T)
+{
+    extern __shared__ __align__(16) unsigned char smraw[];
+    Smem3 &S = *reinterpret_cast<Smem3 *>(smraw);
+    const int lane = threadIdx.x & 31, t = lane % kG3, gbase = lane - t;
+    const int group = threadIdx.x / kG3, ngroups = kThreads3 / kG3;
+    load_consts3(P, 0, S);
+    __syncthreads();
+    const double Bg = P.bgrad[0];
+    const double m = P.mass, dt = T.dt;
+    const double v_rec = P.hbar * P.k / m;
+    const long long ip = (long long)blockIdx.x * ngroups + group;
+    const bool valid = ip < T.n_particles;
+    const long long ipc = valid ? ip : 0;
+    double r[3], vh[3], vs[3], pl;
+    for (int c = 0; c < 3; c++) { r[c] = T.r0[ipc * 3 + c]; vh[c] = T.v0[ipc * 3 + c]; vs[c] = vh[c]; }
+    bool done = !valid;
+    long long na = T.step0 + T.n_steps;
+    long long nev = 0;
+    const long long row = ipc * T.n_steps * 3;
+    if (T.step0 == 0) {
+        if (valid && T.r_traj && t == 0)
+            for (int c = 0; c < 3; c++) { T.r_traj[row + c] = r[c]; T.v_traj[row + c] = vh[c]; }
+        const Out3 o = force3d_point(P, S, S.grp[group], t, gbase, r, vh, Bg, pl);
+        for (int c = 0; c < 3; c++) vh[c] = vh[c] + 0.5 * dt * o.F[c] / m;
+    }
+    const long long j0 = (T.step0 == 0) ? 1 : T.step0;
+    const long long j1 = T.step0 + T.n_steps;
+    for (long long j = j0; j < j1; j++) {
+        if (__all_sync(0xffffffffu, done)) break;
+        double rn[3];
+        for (int c = 0; c < 3; c++) rn[c] = __dadd_rn(r[c], __dmul_rn(dt, vh[c]));  // r + dt v_half
+        const double rr = sqrt(rn[0] * rn[0] + rn[1] * rn[1] + rn[2] * rn[2]);
+        const bool esc = !done && rr > T.r_escape;
+        const Out3 o = force3d_point(P, S, S.grp[group], t, gbase, rn, vh, Bg, pl);
+        if (!done) {
+            for (int c = 0; c < 3; c++) r[c] = rn[c];
+            const long long out_j = j - T.step0;
+            if (esc) {
+                na = j;
+                done = true;
+                for (int c = 0; c < 3; c++) vs[c] = vh[c];
+                if (T.r_traj && t == 0)
+                    for (long long s = out_j; s < T.n_steps; s++)
+                        for (int c = 0; c < 3; c++) {
+                            T.r_traj[row + s * 3 + c] = r[c];
+                            T.v_traj[row + s * 3 + c] = vh[c];
+                        }
+            } else {
+                double vn[3];
+                for (int c = 0; c < 3; c++) vn[c] = vh[c] + dt * o.F[c] / m;
+                if (T.kicks) {
+                    double kick[3];
+                    nev += recoil_kick(T.seed, (unsigned)ip, (unsigned)j, o.R * dt, v_rec, kick);
+                    for (int c = 0; c < 3; c++) vn[c] += kick[c];
+                }
+                for (int c = 0; c < 3; c++) { vs[c] = 0.5 * (vh[c] + vn[c]); vh[c] = vn[c]; }
+                if (T.r_traj && t == 0)
+                    for (int c = 0; c < 3; c++) {
+                        T.r_traj[row + out_j * 3 + c] = r[c];
+                        T.v_traj[row + out_j * 3 + c] = vs[c];
+                    }
+            }
+        }
+    }
+    if (valid && t == 0) {
+        for (int c = 0; c < 3; c++) {
+            T.r_out[ip * 3 + c] = r[c];
+            T.vh_out[ip * 3 + c] = vh[c];
+            if (T.v_out) T.v_out[ip * 3 + c] = vs[c];
+        }
+        T.n_actual[ip] = (int32_t)na;
+        if (T.ke_sum) T.ke_sum[ip] = 0.5 * m * (vs[0] * vs[0] + vs[1] * vs[1] + vs[2] * vs[2]);
+        if (T.n_events) T.n_events[ip] = (int32_t)nev;
+    }
+}
+
+int fill3(const mm_pack *pack, const mm_beams *beams, double hbar, int uniform_fb, Force3Params &P)
+{
+    if (!pack || !beams) { mm_set_error("null pack or beams handle"); return -1; }
+    if (!pack->has3d) { mm_set_error("the molecule pack has no 3D data (Zeeman blocks, |tdm|)"); return -1; }
+    if (!beams->has3d) { mm_set_error("the beam sets have no 3D data (khat)"); return -1; }
+    if (pack->n_g > NGM || pack->n_e > NEM) {
+        mm_set_error("3D kernel supports n_ground <= %d, n_excited <= %d (got %d, %d)", NGM, NEM,
+                     pack->n_g, pack->n_e);
+        return -1;
+    }
+    if (beams->n_b > NBM) { mm_set_error("3D kernel supports <= %d beams", NBM); return -1; }
+    P.n_g = pack->n_g; P.n_e = pack->n_e; P.n_b = beams->n_b; P.n_sets = beams->n_sets;
+    P.Gamma = pack->Gamma; P.k = pack->k; P.mass = pack->mass;
+    P.hbar = hbar > 0 ? hbar : 1.054571817e-34;
+    P.geff = beams->gamma_eff;
+    P.E = pack->buf + pack->oE; P.Zre = pack->buf + pack->oZre; P.Zim = pack->buf + pack->oZim;
+    P.Ze = pack->buf + pack->oZe; P.tdm = pack->buf + pack->oTdm;
+    P.khat = beams->khat; P.freq = beams->freq; P.s0 = beams->s0; P.radius = beams->radius;
+    P.bgrad = beams->bgrad; P.pol = beams->pol;
+    P.uniform_fb = uniform_fb;
+    return 0;
+}
+
+template <class K>
+int prep_smem(K kern)
+{
+    const int sb = (int)sizeof(Smem3);
+    return mm_cuda_check(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, sb),
+                         "cudaFuncSetAttribute") ? -3 : 0;
+}
+
+}  // namespace
+
+extern "C" int mm_force3d_batch(const mm_pack *pack, const mm_beams *beams, const double *r,
+                                const double *v, int64_t n_points, int64_t points_per_set,
+                                double hbar, double *F, double *R, double *pop, int32_t *status,
+                                void *stream)
+{
+    Force3Params P;
+    if (fill3(pack, beams, hbar, 1, P)) return -1;
+    if (!r || !v || !F) { mm_set_error("r, v and F must be non-null"); return -1; }
+    if (n_points < 0) { mm_set_error("n_points < 0"); return -1; }
+    if (n_points == 0) return 0;
+    const long long pps = points_per_set > 0 ? points_per_set : n_points;
+    if ((n_points + pps - 1) / pps > beams->n_sets) {
+        mm_set_error("%lld points at %lld per set need more than %d sets", (long long)n_points, pps,
+                     beams->n_sets);
+        return -1;
+    }
+    P.n_points = n_points; P.pps = pps; P.r = r; P.v = v; P.F = F; P.R = R; P.pop = pop;
+    P.status = status;
+    if (prep_smem(force3d_kernel)) return -3;
+    int dev = 0, nsm = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, force3d_kernel, kThreads3, sizeof(Smem3));
+    const int ngroups = kThreads3 / kG3;
+    const int n_sets_used = (int)((n_points + pps - 1) / pps);
+    long long gx = std::max<long long>(1, (long long)nsm * std::max(per_sm, 1) * 2 / n_sets_used);
+    gx = std::min<long long>(gx, (pps + ngroups - 1) / ngroups);
+    dim3 grid((unsigned)gx, (unsigned)std::min(n_sets_used, 65535));
+    force3d_kernel<<<grid, kThreads3, sizeof(Smem3), (cudaStream_t)stream>>>(P);
+    return mm_cuda_check(cudaGetLastError(), "force3d_kernel launch") ? -3 : 0;
+}
+
+extern "C" int mm_traj3d_run(const mm_pack *pack, const mm_beams *beams, const double *r0,
+                             const double *v0, int64_t n_particles, int64_t step0, int64_t n_steps,
+                             double dt, double r_escape, int32_t kicks, uint64_t seed, double hbar,
+                             double *r_out, double *vh_out, double *v_out, int32_t *n_actual,
+                             double *r_traj, double *v_traj, double *ke, int32_t *n_events,
+                             void *stream)
+{
+    Force3Params P;
+    if (fill3(pack, beams, hbar, 1, P)) return -1;
+    if (!r0 || !v0 || !r_out || !vh_out || !n_actual) {
+        mm_set_error("r0, v0, r_out, vh_out and n_actual must be non-null");
+        return -1;
+    }
+    if ((r_traj == nullptr) != (v_traj == nullptr)) { mm_set_error("r_traj and v_traj go together"); return -1; }
+    if (n_particles < 0 || n_steps < 1 || step0 < 0) {
+        mm_set_error("n_particles >= 0, n_steps >= 1, step0 >= 0 required");
+        return -1;
+    }
+    if (n_particles > 0xffffffffLL || step0 + n_steps > 0xffffffffLL) {
+        mm_set_error("particle and step indices must fit the 32-bit RNG counter words");
+        return -1;
+    }
+    if (n_particles == 0) return 0;
+    P.n_points = 0; P.pps = 1; P.r = P.v = nullptr; P.F = P.R = P.pop = nullptr; P.status = nullptr;
+    Traj3Params T;
+    T.dt = dt; T.r_escape = r_escape; T.n_particles = n_particles; T.n_steps = n_steps;
+    T.step0 = step0; T.kicks = kicks; T.seed = seed;
+    T.r0 = r0; T.v0 = v0; T.r_out = r_out; T.vh_out = vh_out; T.v_out = v_out;
+    T.n_actual = n_actual; T.r_traj = r_traj; T.v_traj = v_traj; T.ke_sum = ke;
+    T.n_events = n_events;
+    if (prep_smem(traj3d_kernel)) return -3;
+    const int ngroups = kThreads3 / kG3;
+    const long long gx = (n_particles + ngroups - 1) / ngroups;
+    traj3d_kernel<<<(unsigned)gx, kThreads3, sizeof(Smem3), (cudaStream_t)stream>>>(P, T);
+    return mm_cuda_check(cudaGetLastError(), "traj3d_kernel launch") ? -3 : 0;
+}

@@ -134,3 +134,34 @@ def capture_velocity_cuda(simulator, z_start=3e-3, v_max=15.0, dv=0.5, dt=1e-6, 
     (molmot_cuda/force_scan_cuda.py:533-670); RF simulators included."""
     from .force_scan import capture_velocity
     return capture_velocity(simulator, z_start, v_max, dv, dt, n_steps, z_escape)
+
+
+# ------------------------------------------------------------------ 3D twins
+def rate_eq_force_3d_batch(mol_data, beams, r_arr, v_arr, B_gradient, Gamma_eff_factor=1.0):
+    """(F [n, 3], R [n], pop [n, n_ground]) -- molmot_cuda/simulator_3d_cuda.py:666-754,
+    with a correct eigensolver."""
+    from .simulator_3d import rate_eq_force_3d_batch as f
+    return f(mol_data, beams, r_arr, v_arr, B_gradient, Gamma_eff_factor)
+
+
+def compute_3d_force_map_cuda(mol_data, beams, axes="xz", n_points=50, v=None, B_gradient=0.0,
+                              extent=5e-3, Gamma_eff_factor=1.0):
+    from .simulator_3d import MOTSimulator3D, compute_3d_force_map
+    sim = MOTSimulator3D(mol_data, list(beams), B_gradient, Gamma_eff_factor=Gamma_eff_factor)
+    return compute_3d_force_map(sim, axes, n_points, v, extent)
+
+
+def simulate_ensemble_3d_cuda(mol_data, beams, r0_list, v0_list, t_max, dt=1e-6, B_gradient=0.0,
+                              Gamma_eff_factor=1.0, r_escape=0.015):
+    """(t [n_steps], r [N, n_steps, 3], v [N, n_steps, 3]) -- one launch for all steps
+    (molmot_cuda/simulator_3d_cuda.py:890-973 launches once per step)."""
+    from .simulator_3d import MOTSimulator3D
+    sim = MOTSimulator3D(mol_data, list(beams), B_gradient, Gamma_eff_factor=Gamma_eff_factor)
+    return sim.simulate_ensemble_arrays(r0_list, v0_list, t_max, dt, r_escape)
+
+
+def simulate_trajectory_3d_cuda(mol_data, beams, r0, v0, t_max, dt=1e-6, B_gradient=0.0,
+                                Gamma_eff_factor=1.0, r_escape=0.015):
+    t, R, V = simulate_ensemble_3d_cuda(mol_data, beams, [r0], [v0], t_max, dt, B_gradient,
+                                        Gamma_eff_factor, r_escape)
+    return t, R[0], V[0]

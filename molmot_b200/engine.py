@@ -279,3 +279,68 @@ def pack_for(mol) -> MoleculePack:
     p = MoleculePack(mol)
     _PACKS[key] = (mol, fp, p)
     return p
+
+
+def beam_sets_3d(khat, freq, q_lab, s0, radius, b_gradient, gamma_eff: float = 1.0) -> BeamSets:
+    """BeamSets carrying unit k vectors and 1/e^2 radii (radius <= 0 or None:
+    plane wave) for the 3D kernels; arrays [n_sets, n_beams(, 3)]."""
+    kh = np.asarray(khat, dtype=np.float64)
+    if kh.ndim == 2:
+        kh = kh[None]
+    n_sets, n_b = kh.shape[:2]
+    rad = np.array([[0.0 if (x is None or not np.isfinite(x)) else float(x) for x in row]
+                    for row in np.asarray(radius, dtype=object).reshape(n_sets, n_b)])
+    return BeamSets(kh[..., 2], np.asarray(freq).reshape(n_sets, n_b),
+                    np.asarray(q_lab).reshape(n_sets, n_b), np.asarray(s0).reshape(n_sets, n_b),
+                    b_gradient, gamma_eff, khat=kh, radius=rad)
+
+
+def force3d_batch(pack: MoleculePack, beams: BeamSets, r, v, *, points_per_set=None,
+                  hbar=None, want_pop=True, stream=None):
+    """3D force at points r[i], v[i] ([n, 3]); dict of device tensors F [n, 3], R, pop, status."""
+    r = _to_dev(r).reshape(-1, 3)
+    v = _to_dev(v).reshape(-1, 3)
+    n = r.shape[0]
+    dev = r.device
+    out = {"F": torch.empty((n, 3), dtype=torch.float64, device=dev),
+           "R": torch.empty(n, dtype=torch.float64, device=dev),
+           "status": torch.empty(n, dtype=torch.int32, device=dev)}
+    if want_pop:
+        out["pop"] = torch.empty((n, pack.n_ground), dtype=torch.float64, device=dev)
+    rc = _lib.load().mm_force3d_batch(pack.handle, beams.handle, _dptr(r), _dptr(v), n,
+                                      int(points_per_set or n), float(hbar or 0.0),
+                                      _dptr(out["F"]), _dptr(out["R"]), _dptr(out.get("pop")),
+                                      _dptr(out["status"]), _stream_handle(stream))
+    _lib.check(rc, "mm_force3d_batch")
+    return out
+
+
+def traj3d(pack: MoleculePack, beams: BeamSets, r0, v0, dt: float, n_steps: int, *, step0: int = 0,
+           r_escape: float = 0.015, kicks: bool = False, seed: int = 0, hbar=None,
+           save_full: bool = False, stream=None):
+    """3D leapfrog ensemble (beam set 0), all steps in one launch.  Returns a
+    dict of device tensors r, vh (half-step velocity; pass both back with
+    step0 to resume), v (synchronised), n_actual, ke, n_events and, with
+    save_full, r_traj / v_traj [N, n_steps, 3]."""
+    r0 = _to_dev(r0).reshape(-1, 3)
+    v0 = _to_dev(v0).reshape(-1, 3)
+    N = r0.shape[0]
+    dev = r0.device
+    f64 = dict(dtype=torch.float64, device=dev)
+    out = {"r": torch.empty((N, 3), **f64), "vh": torch.empty((N, 3), **f64),
+           "v": torch.empty((N, 3), **f64),
+           "n_actual": torch.empty(N, dtype=torch.int32, device=dev),
+           "ke": torch.empty(N, **f64),
+           "n_events": torch.empty(N, dtype=torch.int32, device=dev)}
+    if save_full:
+        out["r_traj"] = torch.empty((N, n_steps, 3), **f64)
+        out["v_traj"] = torch.empty((N, n_steps, 3), **f64)
+    rc = _lib.load().mm_traj3d_run(pack.handle, beams.handle, _dptr(r0), _dptr(v0), N, int(step0),
+                                   int(n_steps), float(dt), float(r_escape), 1 if kicks else 0,
+                                   int(seed) & 0xFFFFFFFFFFFFFFFF, float(hbar or 0.0),
+                                   _dptr(out["r"]), _dptr(out["vh"]), _dptr(out["v"]),
+                                   _dptr(out["n_actual"]), _dptr(out.get("r_traj")),
+                                   _dptr(out.get("v_traj")), _dptr(out["ke"]),
+                                   _dptr(out["n_events"]), _stream_handle(stream))
+    _lib.check(rc, "mm_traj3d_run")
+    return out

@@ -175,6 +175,34 @@ def main():
              r0=np.array(r0s), v0=np.array(v0s), r3=np.array([t[1] for t in tr3]),
              v3=np.array([t[2] for t in tr3]), t_max3=6e-4, z_rf=zrf, v_rf=vrf, t_max_rf=8e-4,
              T_mc=T_mc, mc_n=6, mc_t_max=1.5e-3, mc_t_eq=0.5e-3, versions=ver)
+    # ---- 3D rate-equation force (molmot/mot/simulator_3d.py:168-365) ----
+    from molmot.mot.simulator_3d import MOTSimulator3D, rate_eq_force_3d
+    from molmot.obe.obe_subdoppler import make_beam_pairs_dc4
+    rng3 = np.random.default_rng(3)
+    cases = []
+    for d, sp, s0_, Bg in [(-0.30, 0.40, 1.0, 0.16), (-1.0, 0.7, 3.0, 0.214), (-0.5, 1.2, 0.5, 0.3)]:
+        sim3 = MOTSimulator3D(mol, make_beam_pairs_dc4(mol, d, sp, s0_), B_gradient=Bg)
+        kh = np.array([b.k_hat for b in sim3.beams])
+        fq = np.array([b.freq for b in sim3.beams])
+        ql = np.array([b.q_lab for b in sim3.beams], dtype=np.int32)
+        sb = np.array([b.s0 for b in sim3.beams])
+        rad = np.array([b.beam_radius for b in sim3.beams])
+        r = np.concatenate([np.zeros((1, 3)), rng3.normal(0, 2e-3, (14, 3)),
+                            np.array([[0, 0, 1e-3], [1e-3, 0, 0], [0, 0, -2e-3]])])
+        v = np.concatenate([np.zeros((1, 3)), rng3.normal(0, 1.0, (14, 3)), np.zeros((3, 3))])
+        F = np.zeros((len(r), 3)); R = np.zeros(len(r)); P = np.zeros((len(r), 12))
+        for i in range(len(r)):
+            F[i], R[i], P[i] = rate_eq_force_3d(mol, sim3.beams, r[i], v[i], Bg)
+        cases.append(dict(khat=kh, freq=fq, q=ql, s0=sb, radius=rad, B=Bg, r=r, v=v, F=F, R=R, P=P))
+    np.savez(os.path.join(HERE, "force3d_golden.npz"), versions=ver, n_cases=len(cases),
+             **{f"c{i}_{k}": val for i, c in enumerate(cases) for k, val in c.items()})
+    # short leapfrog trajectories (MOTSimulator3D.simulate_trajectory_3d, :443-504)
+    sim3 = MOTSimulator3D(mol, make_beam_pairs_dc4(mol, -0.30, 0.40, 1.0), B_gradient=0.16)
+    r0s = np.array([[1e-3, -1e-3, 0.5e-3], [0.0, 0.5e-3, -2e-3]])
+    v0s = np.array([[0.3, 0.2, -0.5], [-0.4, 0.0, 0.6]])
+    trs = [sim3.simulate_trajectory_3d(r0s[i], v0s[i], t_max=1.2e-4, dt=1e-6) for i in range(2)]
+    np.savez(os.path.join(HERE, "traj3d_golden.npz"), r0=r0s, v0=v0s, t_max=1.2e-4, dt=1e-6,
+             r=np.array([t[1] for t in trs]), v=np.array([t[2] for t in trs]), versions=ver)
     print("golden fixtures written to", HERE)
 
 
