@@ -121,6 +121,21 @@ MM_API int mm_force_batch(const mm_pack *pack, const mm_beams *beams, const doub
                    const double *z, int64_t n_points, const mm_batch_opts *opts,
                    double *F, double *R, double *pop, int32_t *status, void *stream);
 
+/*
+ * Steady-state force and its gradient with respect to each beam's frequency
+ * and saturation parameter and the set's B' (FP64 form).  Implicit
+ * differentiation through the steady state: one transposed solve per point
+ * with the elimination's own factors (M'^T lambda = dF/dp), on the fixed set
+ * of unclamped populations.  No counterpart in the reference (new on this
+ * path); the reference computes these only by finite differences of
+ * _rate_eq_core.  grad: [n][2 n_beams + 1] rows
+ * (dF/dfreq_b, b = 0..n_beams-1; dF/ds0_b; dF/dB'), Newton per Hz, per unit
+ * s0 and per T/m.  Same layouts as mm_force_batch.
+ */
+MM_API int mm_force_adjoint(const mm_pack *pack, const mm_beams *beams, const double *v,
+                            const double *z, int64_t n_points, const mm_batch_opts *opts,
+                            double *F, double *grad, void *stream);
+
 /* Options of mm_traj_run. */
 typedef struct {
     int32_t ndim;      /* 1: along z; 3: per-axis model of trajectories.py:78-156        */

@@ -71,6 +71,8 @@ SIGNATURES = {
                                      _vp, _vp, _vp, _vp, _vp, _vp]),
     "mm_traj_run": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(TrajOpts), _vp, _vp, ctypes.c_int64,
                                    _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "mm_force_adjoint": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_int64,
+                                        ctypes.POINTER(BatchOpts), _vp, _vp, _vp]),
     "mm_force3d_batch": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_int64, ctypes.c_int64,
                                         ctypes.c_double, _vp, _vp, _vp, _vp, _vp]),
     "mm_traj3d_run": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_int64, ctypes.c_int64,

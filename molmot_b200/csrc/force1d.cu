@@ -76,6 +76,67 @@ force_kernel(ForceParams P)
     }
 }
 
+// Forward force plus its gradient with respect to every beam's frequency and
+// s0 and the set's B' (implicit differentiation through the steady state;
+// the adjoint section of solve_point).  grad row layout per point:
+// [dF/dfreq_0 .. dF/dfreq_{nb-1}, dF/ds0_0 .. dF/ds0_{nb-1}, dF/dB'].
+template <int NGMAX, int NEMAX, int G, bool EXACT>
+__global__ void __launch_bounds__(kThreads, 2)
+force_adjoint_kernel(ForceParams P, double *grad)
+{
+    using GS = GroupShape<NGMAX, NEMAX, G>;
+    extern __shared__ __align__(16) unsigned char sm[];
+    SmemLayout Ly;
+    const int ngroups = kThreads / G;
+    Ly.build(P.n_g, P.n_e, P.n_b, GS::CPL, ngroups, false);
+    const long long pts_per_set = (P.layout == MM_LAYOUT_GRID) ? P.nv * P.nz : P.pps;
+    const int lane = threadIdx.x & 31, t = lane % G, gbase = lane - t;
+    const int group = threadIdx.x / G;
+    double *scr = (double *)(sm + Ly.scratch) + (size_t)group * Ly.scratch_per_group;
+    double *fd = scr, *Ese = scr + P.n_b, *gacc = scr + P.n_b + P.n_e;
+    const int nb = P.n_b, gw = 2 * nb + 1;
+    for (int set = blockIdx.y; set < P.n_sets; set += gridDim.y) {
+        const long long set_first = (long long)set * pts_per_set;
+        long long set_count = pts_per_set;
+        if (set_first + set_count > P.n_points) set_count = P.n_points - set_first;
+        if (set_count <= 0) continue;
+        SetView S;
+        __syncthreads();
+        build_set_tables<G, GS::CPL, false>(P, set, sm, Ly, S);
+        const double Bg = P.bgrad[set];
+        const long long chunk = (set_count + gridDim.x - 1) / gridDim.x;
+        const long long start = (long long)blockIdx.x * chunk;
+        const long long end = min(start + chunk, set_count);
+        for (long long base = start; base < end; base += ngroups) {
+            const long long ip = base + group;
+            const bool valid = ip < end;
+            const long long ipc = valid ? ip : start;
+            double v, z;
+            if (P.layout == MM_LAYOUT_GRID) {
+                v = P.v[ipc / P.nz];
+                z = P.z[ipc % P.nz];
+            } else {
+                v = P.v[set_first + ipc];
+                z = P.z[set_first + ipc];
+            }
+            double xs[GS::CPL];
+            const PointOut o = solve_point<NGMAX, NEMAX, G, false, EXACT, true>(
+                P, S, fd, Ese, t, gbase, v, z, Bg, xs, gacc);
+            if (valid) {
+                const long long gi = set_first + ip;
+                if (t == 0) {
+                    P.F[gi] = o.F;
+                    if (P.R) P.R[gi] = o.R;
+                    if (P.status) P.status[gi] = o.status;
+                    grad[gi * gw + 2 * nb] = o.gB;
+                }
+                for (int i = t; i < 2 * nb; i += G) grad[gi * gw + i] = gacc[i];
+            }
+            __syncwarp();
+        }
+    }
+}
+
 struct TrajParams {
     double dt, z_escape, mass;
     long long n_particles, n_steps;
@@ -232,6 +293,30 @@ int launch_force(const ForceParams &P, long long pts_per_set, cudaStream_t st)
     return mm_cuda_check(cudaGetLastError(), "force_kernel launch") ? -3 : 0;
 }
 
+template <class C>
+int launch_adjoint(const ForceParams &P, double *grad, cudaStream_t st)
+{
+    auto kern = force_adjoint_kernel<C::ng, C::ne, C::g, C::exact>;
+    const size_t sb = smem_bytes<C, false>(P);
+    if (sb > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb);
+        if (mm_cuda_check(e, "cudaFuncSetAttribute")) return -3;
+    }
+    int dev = 0, nsm = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, sb);
+    if (per_sm < 1) per_sm = 1;
+    const int ngroups = kThreads / C::g;
+    const long long pts_per_set = (P.layout == MM_LAYOUT_GRID) ? P.nv * P.nz : P.pps;
+    const long long want = (long long)nsm * per_sm * 4;
+    long long gx = std::max<long long>(1, want / std::max(1, P.n_sets));
+    gx = std::min(gx, std::max<long long>(1, (pts_per_set + ngroups - 1) / ngroups));
+    dim3 grid((unsigned)gx, (unsigned)std::min(P.n_sets, 65535));
+    kern<<<grid, kThreads, sb, st>>>(P, grad);
+    return mm_cuda_check(cudaGetLastError(), "force_adjoint_kernel launch") ? -3 : 0;
+}
+
 template <class C, bool FP32>
 int launch_traj(const ForceParams &P, const TrajParams &T, cudaStream_t st)
 {
@@ -280,11 +365,31 @@ int fill_params(const mm_pack *pack, const mm_beams *beams, const mm_batch_opts 
 
 }  // namespace
 
-extern "C" int mm_force_batch(const mm_pack *pack, const mm_beams *beams, const double *v,
-                              const double *z, int64_t n_points, const mm_batch_opts *opts,
-                              double *F, double *R, double *pop, int32_t *status, void *stream)
+static int prepare_batch(const mm_pack *pack, const mm_beams *beams, const double *v,
+                         const double *z, int64_t n_points, const mm_batch_opts *opts, double *F,
+                         ForceParams &P, long long &pps);
+
+extern "C" int mm_force_adjoint(const mm_pack *pack, const mm_beams *beams, const double *v,
+                                const double *z, int64_t n_points, const mm_batch_opts *opts,
+                                double *F, double *grad, void *stream)
 {
     ForceParams P;
+    long long pps;
+    const int rc = prepare_batch(pack, beams, v, z, n_points, opts, F, P, pps);
+    if (rc <= 0) return rc;
+    if (!grad) { mm_set_error("grad must be non-null"); return -1; }
+    if (opts->precision != MM_PREC_FP64) { mm_set_error("the adjoint runs in the FP64 form only"); return -1; }
+    P.R = nullptr; P.pop = nullptr; P.status = nullptr;
+    cudaStream_t st = (cudaStream_t)stream;
+    return dispatch_class(P.n_g, P.n_e, [&](auto C) -> int { return launch_adjoint<decltype(C)>(P, grad, st); });
+}
+
+// Validates a batch call and fills P; returns 1 to launch, 0 for an empty
+// batch, < 0 on error.
+static int prepare_batch(const mm_pack *pack, const mm_beams *beams, const double *v,
+                         const double *z, int64_t n_points, const mm_batch_opts *opts, double *F,
+                         ForceParams &P, long long &pps)
+{
     if (fill_params(pack, beams, opts, P)) return -1;
     if (!opts) { mm_set_error("opts is required"); return -1; }
     if (!v || !z || !F) { mm_set_error("v, z and F must be non-null"); return -1; }
@@ -292,7 +397,6 @@ extern "C" int mm_force_batch(const mm_pack *pack, const mm_beams *beams, const 
     if (n_points == 0) return 0;
     P.layout = opts->layout;
     P.nv = opts->nv; P.nz = opts->nz; P.pps = opts->points_per_set;
-    long long pps;
     if (opts->layout == MM_LAYOUT_GRID) {
         if (opts->nv < 1 || opts->nz < 1) { mm_set_error("grid layout needs nv, nz >= 1"); return -1; }
         pps = opts->nv * opts->nz;
@@ -313,10 +417,25 @@ extern "C" int mm_force_batch(const mm_pack *pack, const mm_beams *beams, const 
         mm_set_error("unknown layout %d", opts->layout);
         return -1;
     }
+    if (opts->precision != MM_PREC_FP64 && opts->precision != MM_PREC_FP32_REFINE) {
+        mm_set_error("unknown precision %d", opts->precision);
+        return -1;
+    }
     P.n_points = n_points;
-    P.v = v; P.z = z; P.F = F; P.R = R; P.pop = pop; P.status = status;
+    P.v = v; P.z = z; P.F = F;
+    return 1;
+}
+
+extern "C" int mm_force_batch(const mm_pack *pack, const mm_beams *beams, const double *v,
+                              const double *z, int64_t n_points, const mm_batch_opts *opts,
+                              double *F, double *R, double *pop, int32_t *status, void *stream)
+{
+    ForceParams P;
+    long long pps;
+    const int prc = prepare_batch(pack, beams, v, z, n_points, opts, F, P, pps);
+    if (prc <= 0) return prc;
+    P.R = R; P.pop = pop; P.status = status;
     const bool fp32 = opts->precision == MM_PREC_FP32_REFINE;
-    if (opts->precision != MM_PREC_FP64 && !fp32) { mm_set_error("unknown precision %d", opts->precision); return -1; }
     cudaStream_t st = (cudaStream_t)stream;
     return dispatch_class(P.n_g, P.n_e, [&](auto C) -> int {
         using CT = decltype(C);

@@ -91,11 +91,12 @@ struct SetView {
     const int *cnt, *off, *maxcnt;    // per ground state / per slot
     const Trip64 *t64;
     const Trip32 *t32;
+    const double *d2t;                // |d|^2 of each FP64 triple (adjoint)
 };
 
 // Byte layout of the dynamic shared memory of the 1D force kernels.
 struct SmemLayout {
-    size_t E, zd, czd, BR, freq, ck, cnt, off, maxcnt, trip, scratch, total;
+    size_t E, zd, czd, BR, freq, ck, cnt, off, maxcnt, trip, d2t, scratch, total;
     int ntrip_max, scratch_per_group;  // doubles per group
 
     __host__ __device__ static size_t al(size_t x) { return (x + 15) & ~size_t(15); }
@@ -115,7 +116,9 @@ struct SmemLayout {
         maxcnt = o; o = al(o + sizeof(int) * cpl);
         ntrip_max = n_g * n_b * n_e;
         trip = o; o = al(o + (fp32 ? sizeof(Trip32) : sizeof(Trip64)) * (size_t)ntrip_max);
-        scratch_per_group = fp32 ? 0 : n_b + n_e;
+        d2t = o; o = al(o + sizeof(double) * (size_t)(fp32 ? 0 : ntrip_max));
+        // FP64 form: doppler-shifted frequencies, excited energies, adjoint accumulators
+        scratch_per_group = fp32 ? 0 : n_b + n_e + 2 * n_b;
         scratch = o; o = al(o + sizeof(double) * (size_t)scratch_per_group * ngroups);
         total = o;
     }
@@ -133,6 +136,7 @@ __device__ void build_set_tables(const ForceParams &P, int set, unsigned char *s
     int *cnt = (int *)(sm + Ly.cnt), *off = (int *)(sm + Ly.off), *maxcnt = (int *)(sm + Ly.maxcnt);
     Trip64 *t64 = (Trip64 *)(sm + Ly.trip);
     Trip32 *t32 = (Trip32 *)(sm + Ly.trip);
+    double *d2t = (double *)(sm + Ly.d2t);
     const int tid = threadIdx.x, nt = blockDim.x;
     const double *kdir = P.kdir + (size_t)set * n_b, *fr = P.freq + (size_t)set * n_b;
     const double *s0 = P.s0 + (size_t)set * n_b;
@@ -187,6 +191,7 @@ __device__ void build_set_tables(const ForceParams &P, int set, unsigned char *s
                     tr.hk = hk;
                     tr.be = b | (e << 8);
                     tr.pad = 0;
+                    d2t[o] = d2;
                     t64[o++] = tr;
                 } else {
                     Trip32 tr;
@@ -204,13 +209,14 @@ __device__ void build_set_tables(const ForceParams &P, int set, unsigned char *s
     }
     __syncthreads();
     S.E = E; S.zd = zd; S.czd = czd; S.BR = BR; S.freq = freq; S.ck = ck;
-    S.cnt = cnt; S.off = off; S.maxcnt = maxcnt; S.t64 = t64; S.t32 = t32;
+    S.cnt = cnt; S.off = off; S.maxcnt = maxcnt; S.t64 = t64; S.t32 = t32; S.d2t = d2t;
 }
 
 // Result of one point, identical in every lane of the group.
 struct PointOut {
     double F, R;
     int status;
+    double gB;  // dF/dB' (adjoint variant only)
 };
 
 template <int NGMAX, int NEMAX, int G>
@@ -222,11 +228,12 @@ struct GroupShape {
 // fd / Ese: this group's scratch (n_b + n_e doubles) in shared memory
 // (FP64 form only).  EXACT: the molecule has exactly NGMAX ground and NEMAX
 // excited states (size predicates vanish at compile time).
-template <int NGMAX, int NEMAX, int G, bool FP32, bool EXACT>
+template <int NGMAX, int NEMAX, int G, bool FP32, bool EXACT, bool ADJ = false>
 __device__ __forceinline__ PointOut solve_point(const ForceParams &P, const SetView &S, double *fd,
                                                 double *Ese, int t, int gbase, double v, double z,
                                                 double Bgrad,
-                                                double (&xs)[GroupShape<NGMAX, NEMAX, G>::CPL])
+                                                double (&xs)[GroupShape<NGMAX, NEMAX, G>::CPL],
+                                                double *gacc = nullptr)
 {
     constexpr int CPL = GroupShape<NGMAX, NEMAX, G>::CPL;
     constexpr unsigned FULL = 0xffffffffu;
@@ -238,7 +245,7 @@ __device__ __forceinline__ PointOut solve_point(const ForceParams &P, const SetV
 
     // ---------------- rates of the owned ground states ----------------
     double R[CPL][NEMAX];
-    double Fk[CPL], Rk[CPL];
+    double Fk[CPL], Rk[CPL], satk[CPL];
     const double B_gauss = __dmul_rn(__dmul_rn(Bgrad, z), 1e4);
     if (!FP32) {
         __syncwarp();
@@ -286,6 +293,7 @@ __device__ __forceinline__ PointOut solve_point(const ForceParams &P, const SetV
             }
             // saturation correction 1/(1 + s_total[g]) (rate_equations_jit.py:85-90)
             const double sat = mm_rcp(1.0 + s);
+            satk[c] = sat;
             double rs = 0.0;
 #pragma unroll
             for (int e = 0; e < NEMAX; e++) {
@@ -574,6 +582,116 @@ __device__ __forceinline__ PointOut solve_point(const ForceParams &P, const SetV
     PointOut out;
     out.F = mm_group_sum(F, G);
     out.R = mm_group_sum(Rs, G);
+    out.gB = 0.0;
+    if constexpr (ADJ && !FP32) {
+        // ---------- adjoint: dF/dtheta = sum_{b,g,e} (p_g hk_b - mu[g,e]) d rate_bge / dtheta ----------
+        // with lambda solving M'^T lambda = dF/dp = F_g and
+        // mu[g,e] = p_g (sum_{g'<n-1} lambda_g' BR[e,g'] - lambda_g [g<n-1]) (implicit differentiation
+        // of M' p = e_last on the fixed active set; the last row of M' is constant).
+        // Transposed solve with the stored factors, P M' = L U:  U^T w = F, L^T u = w, lambda = P^T u.
+        double wv[NGMAX];
+        static_for<0, NGMAX>([&](auto ic) {
+            constexpr int i = decltype(ic)::value;
+            constexpr int own = i % G, li = i / G;
+            double wi = 0.0;
+            if (EXACT || i < n_g) {
+                if (t == own) {
+                    double sacc = Fk[li];
+#pragma unroll
+                    for (int j = 0; j < i; j++) sacc = fma(-A[li][j], wv[j], sacc);  // U[j][i]
+                    wi = sacc * invU[li];
+                }
+                wi = __shfl_sync(FULL, wi, gbase + own);
+            }
+            wv[i] = wi;
+        });
+        static_for<0, NGMAX>([&](auto iic) {
+            constexpr int i = NGMAX - 1 - decltype(iic)::value;
+            constexpr int own = i % G, li = i / G;
+            if (EXACT || i < n_g) {
+                double ui = 0.0;
+                if (t == own) {
+                    double sacc = wv[i];
+#pragma unroll
+                    for (int j = i + 1; j < NGMAX; j++)
+                        if (EXACT || j < n_g) sacc = fma(-A[li][j], wv[j], sacc);  // L[j][i]
+                    ui = sacc;
+                }
+                wv[i] = __shfl_sync(FULL, ui, gbase + own);
+            }
+        });
+        if (__any_sync(FULL, swapped)) {
+#pragma unroll
+            for (int col = NGMAX - 1; col >= 0; col--) {
+#pragma unroll
+                for (int r = col + 1; r < NGMAX; r++)
+                    if (r == prows[col]) { const double tmp = wv[col]; wv[col] = wv[r]; wv[r] = tmp; }
+            }
+        }
+        double nu[NEMAX];
+#pragma unroll
+        for (int e = 0; e < NEMAX; e++) {
+            double a = 0.0;
+#pragma unroll
+            for (int g = 0; g < NGMAX; g++)
+                if (g < n_g - 1 && e < n_e) a = fma(wv[g], S.BR[e * n_g + g], a);
+            nu[e] = a;
+        }
+        // per-beam accumulators (this group's shared scratch): dF/dfreq_b, dF/ds0_b
+        for (int i = t; i < 2 * P.n_b; i += G) gacc[i] = 0.0;
+        __syncwarp();
+        const double geff = P.geff;
+        double gB = 0.0;
+#pragma unroll
+        for (int c = 0; c < CPL; c++) {
+            const int k = c * G + t;
+            const bool own = EXACT ? (k < NGMAX) : (k < n_g);
+            const int kk = own ? k : 0;
+            const int cntk = own ? S.cnt[kk] : 0;
+            const int o = S.off[kk];
+            const int mc = S.maxcnt[c];
+            double lamk = 0.0;
+#pragma unroll
+            for (int g = c * G; g < c * G + G && g < NGMAX; g++)
+                if (g == k) lamk = wv[g];
+            const double pk = xs[c], sat = satk[c];
+            double mu[NEMAX];
+#pragma unroll
+            for (int e = 0; e < NEMAX; e++) mu[e] = pk * (nu[e] - ((k < n_g - 1) ? lamk : 0.0));
+            const double Esg = fma(B_gauss, S.czd[kk], S.E[kk]);
+            double T = 0.0;
+            for (int pass = 0; pass < 2; pass++) {
+                const double C = T * sat;
+                for (int i = 0; i < mc; i++) {
+                    if (i < cntk) {
+                        const Trip64 tr = S.t64[o + i];
+                        const int b = tr.be & 0xff, e = tr.be >> 8;
+                        const double om = __dsub_rn(Ese[e], Esg);
+                        const double de = __dmul_rn(__dsub_rn(fd[b], om), MM_TWO_PI);
+                        const double L = gh2 * mm_rcp(fma(de, de, gh2));
+                        const double rate = tr.c1g * L * sat;
+                        double mue = 0.0;
+#pragma unroll
+                        for (int ee = 0; ee < NEMAX; ee++)
+                            if (ee == e) mue = mu[ee];
+                        const double w = pk * tr.hk - mue;
+                        if (pass == 0) {
+                            T = fma(w, rate, T);
+                        } else {
+                            const double Q = w * rate - C * tr.c2 * L;
+                            const double dLL = -2.0 * de * L / gh2;  // (dL/d delta) / L
+                            atomicAdd(&gacc[b], Q * dLL * MM_TWO_PI);
+                            atomicAdd(&gacc[P.n_b + b], S.d2t[o + i] * L * (w * gh * geff * sat - C));
+                            const double ddB = -z * 1e4 * (S.zd[n_g + e] - S.zd[kk]) * P.Gamma;
+                            gB = fma(Q * dLL, ddB, gB);
+                        }
+                    }
+                }
+            }
+        }
+        out.gB = mm_group_sum(gB, G);
+        __syncwarp();
+    }
     if (!isfinite(out.F)) stat |= MM_ST_NONFINITE;
     out.status = mm_group_or(stat, G);
     return out;

@@ -1,0 +1,116 @@
+"""Adjoint gradients of the steady-state force (mm_force_adjoint) and of the
+MOT coefficients k, beta (33-point stencils) with respect to the 4
+detunings, 4 powers (s0) and B'.
+
+Checks:
+  * against FP64 torch autograd of a dense restatement (oracle/torch_dense.py)
+    -- tolerance 1e-8 of the largest gradient component per parameter set;
+  * against central finite differences of the GPU forward with
+    h = 1e-4 relative -- tolerance 1e-5 relative.
+"""
+import numpy as np
+import pytest
+import torch
+
+from conftest import golden
+
+pytestmark = pytest.mark.gpu
+
+
+def _sets(mol, n_sets, seed):
+    """Parameter sets as in the batched-map workload: 4 detunings in [-40, 0] MHz,
+    per-frequency s0 log-uniform in [0.1, 10], B' in [5, 40] G/cm."""
+    rng = np.random.default_rng(seed)
+    E = mol.energies
+    ref = np.array([E[15] - E[0], E[15] - E[0], E[15] - E[9], E[15] - E[9]])
+    det = rng.uniform(-40e6, 0.0, (n_sets, 4))
+    s0 = 10 ** rng.uniform(-1, 1, (n_sets, 4))
+    B = rng.uniform(5, 40, n_sets) * 1e-2
+    pols = np.array([2, 0, 2, 0])
+    kdir = np.tile([1.0, -1.0], (n_sets, 4))
+    pol = np.tile(np.stack([pols, 2 - pols], 1).ravel(), (n_sets, 1))
+    return ref, det, s0, B, kdir, pol
+
+
+def _params(ref, det, s0, B, dev):
+    f = torch.tensor(det, dtype=torch.float64, device=dev, requires_grad=True)
+    p = torch.tensor(s0, dtype=torch.float64, device=dev, requires_grad=True)
+    b = torch.tensor(B, dtype=torch.float64, device=dev, requires_grad=True)
+    freq = (torch.as_tensor(ref, dtype=torch.float64, device=dev)[None, :] + f).repeat_interleave(2, 1)
+    s0b = p.repeat_interleave(2, 1)
+    return f, p, b, freq, s0b
+
+
+def test_adjoint_vs_torch_autograd(mol, gpu):
+    from molmot_b200.autograd import steady_state_force
+    from oracle import torch_dense as td
+    ref, det, s0, B, kdir, pol = _sets(mol, 6, 1)
+    rng = np.random.default_rng(2)
+    pps = 40
+    v = rng.uniform(-10, 10, 6 * pps)
+    z = rng.uniform(-1e-2, 1e-2, 6 * pps)
+    w = torch.as_tensor(rng.normal(size=6 * pps), dtype=torch.float64)
+    f1, p1, b1, freq1, s01 = _params(ref, det, s0, B, gpu)
+    F1 = steady_state_force(mol, kdir, pol, freq1, s01, b1, v, z, pps)
+    (F1.cpu() * w).sum().backward()
+    f2, p2, b2, freq2, s02 = _params(ref, det, s0, B, "cpu")
+    F2 = td.force(mol, kdir, pol, freq2, s02, b2, v, z, pps)
+    assert np.abs(F1.detach().cpu().numpy() - F2.detach().numpy()).max() < 1e-10 * F2.abs().max().item()
+    (F2 * w).sum().backward()
+    for a, b in [(f1, f2), (p1, p2), (b1, b2)]:
+        ga, gb = a.grad.cpu().numpy(), b.grad.numpy()
+        scale = np.abs(gb).max(axis=-1, keepdims=True) if gb.ndim > 1 else np.abs(gb).max()
+        assert np.all(np.abs(ga - gb) <= 1e-8 * scale + 1e-300), (ga, gb)
+
+
+def test_mot_coefficient_gradients_vs_central_fd(mol, gpu):
+    from molmot_b200.autograd import mot_coefficients
+    ref, det, s0, B, kdir, pol = _sets(mol, 4, 3)
+    f, p, b, freq, s0b = _params(ref, det, s0, B, gpu)
+    k, beta = mot_coefficients(mol, kdir, pol, freq, s0b, b)
+    gk = torch.autograd.grad(k.sum(), [f, p, b], retain_graph=True)
+    gbeta = torch.autograd.grad(beta.sum(), [f, p, b])
+
+    def kb(det_, s0_, B_):
+        with torch.no_grad():
+            _, _, _, fr, s0bb = _params(ref, det_, s0_, B_, gpu)
+            bb = torch.tensor(B_, dtype=torch.float64, device=gpu)
+            kk, be = mot_coefficients(mol, kdir, pol, fr, s0bb, bb)
+        return kk.cpu().numpy(), be.cpu().numpy()
+
+    for which, base in [(0, det), (1, s0), (2, B)]:
+        for idx in np.ndindex(base.shape[1:] if base.ndim > 1 else ()):
+            h = 1e-4 * np.abs(base[(slice(None),) + idx])
+            args_p = [det.copy(), s0.copy(), B.copy()]
+            args_m = [det.copy(), s0.copy(), B.copy()]
+            args_p[which][(slice(None),) + idx] += h
+            args_m[which][(slice(None),) + idx] -= h
+            kp, bp = kb(*args_p)
+            km, bm = kb(*args_m)
+            if which == 0:
+                # a detuning enters as the absolute frequency ref + det (~4.3e14 Hz, ulp
+                # 0.0625 Hz): divide by the step the frequencies actually took
+                i0 = idx[0]
+                h = ((ref[i0] + args_p[0][:, i0]) - (ref[i0] + args_m[0][:, i0])) / 2
+            fd_k = (kp - km) / (2 * h)
+            fd_b = (bp - bm) / (2 * h)
+            ad_k = gk[which].cpu().numpy()[(slice(None),) + idx]
+            ad_b = gbeta[which].cpu().numpy()[(slice(None),) + idx]
+            # relative to the largest sensitivity of each coefficient in the set
+            sk = np.max(np.abs(gk[which].cpu().numpy().reshape(4, -1) * base.reshape(4, -1)), axis=1)
+            sb = np.max(np.abs(gbeta[which].cpu().numpy().reshape(4, -1) * base.reshape(4, -1)), axis=1)
+            scale = np.abs(base[(slice(None),) + idx])
+            assert np.all(np.abs(fd_k - ad_k) * scale <= 1e-5 * sk), (which, idx)
+            assert np.all(np.abs(fd_b - ad_b) * scale <= 1e-5 * sb), (which, idx)
+
+
+def test_adjoint_forward_equals_force_batch(mol, gpu):
+    from molmot_b200.engine import BeamSets, force_batch, force_adjoint, pack_for
+    g = golden("random_points.npz")
+    ns, npts = int(g["n_sets"]), int(g["n_pts"])
+    sel = lambda a: a.reshape(ns, npts, *a.shape[1:])[:, 0]
+    bs = BeamSets(sel(g["kdir"]), sel(g["freq"]), sel(g["pol"]), sel(g["s0"]), sel(g["B"]))
+    F, G = force_adjoint(pack_for(mol), bs, g["v"], g["z"], points_per_set=npts)
+    F2 = force_batch(pack_for(mol), bs, g["v"], g["z"], points_per_set=npts)["F"]
+    assert torch.equal(F, F2)
+    assert G.shape == (ns * npts, 17)
