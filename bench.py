@@ -145,6 +145,62 @@ def cpu_baseline(mol, n_sets_sample=8):
                       f"prange over points, os.cpu_count()={os.cpu_count()}"}
 
 
+def _ev_time(torch, fn, reps=3):
+    fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def secondary_measurements(torch, mol, pack, dev):
+    """Particle-steps/s of the trajectory ensembles and the adjoint's cost."""
+    from molmot_b200.engine import BeamSets, force_batch, force_adjoint, traj
+    from molmot_b200.fields import make_dc_mot_beams
+    from molmot_b200.simulator_3d import MOTSimulator3D, make_beam_pairs_dc4
+    out = {}
+    rng = np.random.default_rng(SEED)
+    # 3D quadrupole MOT, 24 beams, 65,536 particles: r ~ N(0, 1 mm), v ~ MB(5 mK), kicks on
+    N3, S3 = 65536, 24
+    sim3 = MOTSimulator3D(mol, make_beam_pairs_dc4(mol, -0.30, 0.40, 1.0), B_gradient=0.16)
+    sig_v = float(np.sqrt(1.380649e-23 * 5e-3 / mol.mass))
+    r0 = torch.as_tensor(rng.normal(0, 1e-3, (N3, 3)), device=dev)
+    v0 = torch.as_tensor(rng.normal(0, sig_v, (N3, 3)), device=dev)
+    ms = _ev_time(torch, lambda: sim3.run_ensemble(r0, v0, S3 * 1e-6, kicks=True, seed=SEED), 2)
+    ps = N3 * S3 / (ms * 1e-3)
+    out["traj3d"] = {"metric": "particle-steps/s", "value": ps, "particles": N3, "steps": S3,
+                     "ms": ms, "workload": "SrOH 3D quadrupole MOT, 24 beams, leapfrog dt=1us, "
+                     "Philox recoil kicks, FP64 state; full 65,536 x 30,000-step run "
+                     f"extrapolates to {N3 * 30000 / ps:.0f} s"}
+    # 1D DC MOT ensemble (the reference's trajectory configuration), 65,536 particles
+    bs1 = BeamSets.from_beams(make_dc_mot_beams(mol, -0.20, 0.70, 1.0), 0.16)
+    z0 = torch.as_tensor(rng.normal(0, 2e-3, 65536), device=dev)
+    u0 = torch.as_tensor(rng.normal(0, 1.0, 65536), device=dev)
+    S1 = 1000
+    ms = _ev_time(torch, lambda: traj(pack, bs1, z0, u0, 1e-6, S1), 2)
+    out["traj1d"] = {"metric": "particle-steps/s", "value": 65536 * (S1 - 1) / (ms * 1e-3),
+                     "particles": 65536, "steps": S1, "ms": ms,
+                     "workload": "SrOH 1D DC MOT (delta -0.2, split 0.7, s0 1, B' 0.16 T/m), Euler"}
+    # adjoint: 1024 parameter sets x 66 stencil points (33 z + 33 v)
+    kdir, freq, pol, s0, B = make_params(mol, 1024, SEED + 7)
+    bsa = BeamSets(kdir, freq, pol, s0, B)
+    zs = np.linspace(-0.3e-3, 0.3e-3, 33)
+    vs = np.linspace(-0.1, 0.1, 33)
+    v = torch.as_tensor(np.tile(np.concatenate([np.zeros(33), vs]), 1024), device=dev)
+    z = torch.as_tensor(np.tile(np.concatenate([zs, np.zeros(33)]), 1024), device=dev)
+    tf = _ev_time(torch, lambda: force_batch(pack, bsa, v, z, points_per_set=66, want_pop=False,
+                                             want_R=False, want_status=False), 5)
+    ta = _ev_time(torch, lambda: force_adjoint(pack, bsa, v, z, points_per_set=66), 5)
+    out["adjoint"] = {"workload": "1024 parameter sets x (33 z + 33 v) stencil points, gradients "
+                                  "w.r.t. 8 beam frequencies, 8 s0 and B'",
+                      "forward_ms": tf, "forward_plus_adjoint_ms": ta, "cost_ratio": ta / tf}
+    return out
+
+
 def oracle_check(mol, pack, bs, v_d, z_d, kdir, freq, pol, s0, B, sets=(0, 1, 2047, 4095)):
     """Both GPU forms against the CPU oracle on a few whole sets (the checker;
     part of the cpu_baseline leg, rank 0 only)."""
@@ -316,6 +372,8 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     ms_e2e = float(t.item())
 
+    secondary = secondary_measurements(torch, mol, pack, dev) if world == 1 else None
+
     A = active_triples(mol.d_squared, pol[0])
     f64_32, f32_32 = flops_per_point(12, 4, 8, A, refine=True)
     f64_64, _ = flops_per_point(12, 4, 8, A, refine=False)
@@ -356,6 +414,7 @@ def main():
                     "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                     "ms_per_step": ms_e2e},
             "accuracy": accuracy,
+            "secondary": secondary,
             "gpu_launches": args.steps * 2,
             "clocks": clk,
         }
