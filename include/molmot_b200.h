@@ -136,6 +136,40 @@ MM_API int mm_force_adjoint(const mm_pack *pack, const mm_beams *beams, const do
                             const double *z, int64_t n_points, const mm_batch_opts *opts,
                             double *F, double *grad, void *stream);
 
+/*
+ * Uneven batches: many different molecules (n_ground 2..48, n_excited 1..16),
+ * each with its own beam set and number of points.  No single counterpart in
+ * the reference, which handles one molecule per CUDAMolData
+ * (molmot_cuda/rate_equations_cuda.py:399-441) and launches per call.
+ */
+typedef struct mm_bank mm_bank;
+typedef struct mm_uneven_plan mm_uneven_plan;
+
+/* Upload n_mol molecules (1D fields of mm_mol_desc) into one device bank. */
+MM_API int mm_bank_create(const mm_mol_desc *mols, int32_t n_mol, mm_bank **out);
+MM_API int mm_bank_destroy(mm_bank *bank);
+
+typedef struct {
+    int32_t warps_per_cta[3]; /* per size class (n_g <= 16, <= 32, <= 48); <= 0: default */
+    int32_t chunk_groups;     /* points per work item, in CTA widths; <= 0: 8          */
+} mm_uneven_opts;
+
+/* Work plan: molecule m owns points [point_offsets[m], point_offsets[m+1])
+ * (host array of n_mol + 1).  Allocates the plan's task lists and counters. */
+MM_API int mm_uneven_plan_create(const mm_bank *bank, const int64_t *point_offsets,
+                                 const mm_uneven_opts *opts, mm_uneven_plan **out);
+MM_API int mm_uneven_plan_destroy(mm_uneven_plan *plan);
+
+/* Forces of every point (device arrays v, z, F [n], R and status nullable).
+ * beams: one set per molecule.  persistent = 1: one persistent launch per
+ * size class drawing work items from the plan's counters (reset on `stream`
+ * by this call, so the whole call can be captured in a CUDA graph);
+ * persistent = 0: one CTA per work item.  hbar <= 0: 1.0545718e-34. */
+MM_API int mm_uneven_force(const mm_uneven_plan *plan, const mm_beams *beams, const double *v,
+                           const double *z, double hbar, int32_t uniform_fallback,
+                           int32_t persistent, double *F, double *R, int32_t *status,
+                           void *stream);
+
 /* Options of mm_traj_run. */
 typedef struct {
     int32_t ndim;      /* 1: along z; 3: per-axis model of trajectories.py:78-156        */

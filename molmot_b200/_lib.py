@@ -56,6 +56,10 @@ class TrajOpts(ctypes.Structure):
                 ("hbar", ctypes.c_double)]
 
 
+class UnevenOpts(ctypes.Structure):
+    _fields_ = [("warps_per_cta", ctypes.c_int32 * 3), ("chunk_groups", ctypes.c_int32)]
+
+
 #: every symbol include/molmot_b200.h declares, with (restype, argtypes)
 SIGNATURES = {
     "mm_last_error": (ctypes.c_char_p, []),
@@ -79,6 +83,13 @@ SIGNATURES = {
                                      ctypes.c_int64, ctypes.c_double, ctypes.c_double,
                                      ctypes.c_int32, ctypes.c_uint64, ctypes.c_double,
                                      _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "mm_bank_create": (ctypes.c_int, [ctypes.POINTER(MolDesc), ctypes.c_int32, ctypes.POINTER(_vp)]),
+    "mm_bank_destroy": (ctypes.c_int, [_vp]),
+    "mm_uneven_plan_create": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int64),
+                                             ctypes.POINTER(UnevenOpts), ctypes.POINTER(_vp)]),
+    "mm_uneven_plan_destroy": (ctypes.c_int, [_vp]),
+    "mm_uneven_force": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_double, ctypes.c_int32,
+                                       ctypes.c_int32, _vp, _vp, _vp, _vp]),
     "mm_peak_probe": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int64, _dp, _dp, _vp]),
 }
 
