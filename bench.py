@@ -268,6 +268,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--sets", type=int, default=N_SETS, help="parameter sets per GPU")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-secondary", action="store_true",
+                    help="skip the trajectory / adjoint measurements (small profiling runs)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -372,7 +374,8 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     ms_e2e = float(t.item())
 
-    secondary = secondary_measurements(torch, mol, pack, dev) if world == 1 else None
+    secondary = (secondary_measurements(torch, mol, pack, dev)
+                 if world == 1 and not args.no_secondary else None)
 
     A = active_triples(mol.d_squared, pol[0])
     f64_32, f32_32 = flops_per_point(12, 4, 8, A, refine=True)
