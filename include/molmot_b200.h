@@ -170,6 +170,29 @@ MM_API int mm_uneven_force(const mm_uneven_plan *plan, const mm_beams *beams, co
                            int32_t persistent, double *F, double *R, int32_t *status,
                            void *stream);
 
+/*
+ * mm_uneven_force_static: the same forces as mm_uneven_force (persistent = 1)
+ * with no plan and no allocation of any kind.  It has no counterpart in the
+ * reference.  It is for callers that cannot allocate when they ask for
+ * forces: a point layout that changes every call (adaptive sampling, an
+ * ensemble losing particles) would otherwise create and destroy a plan per
+ * call, and cudaFree synchronises the whole device; a host application that
+ * has handed the device memory to its own pool has none left to allocate.
+ * The work list and work counters live in a fixed 1 MiB array in the
+ * library's device memory (per GPU), so a batch may make at most 43,680 work
+ * items (point chunks of chunk_groups CTA widths); a larger one is refused
+ * with an error naming the limit.  The counters are zeroed on `stream` by
+ * every call.  The first call on each GPU looks up the array's device
+ * address (cudaGetSymbolAddress); it must come before any stream capture on
+ * that GPU.  Calls share the array and host staging arrays: calls that
+ * overlap in time (two host threads, or two streams of one GPU) race.
+ */
+MM_API int mm_uneven_force_static(const mm_bank *bank, const mm_beams *beams,
+                                  const int64_t *point_offsets, const mm_uneven_opts *opts,
+                                  const double *v, const double *z, double hbar,
+                                  int32_t uniform_fallback, double *F, double *R,
+                                  int32_t *status, void *stream);
+
 /* Options of mm_traj_run. */
 typedef struct {
     int32_t ndim;      /* 1: along z; 3: per-axis model of trajectories.py:78-156        */

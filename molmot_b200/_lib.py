@@ -90,6 +90,9 @@ SIGNATURES = {
     "mm_uneven_plan_destroy": (ctypes.c_int, [_vp]),
     "mm_uneven_force": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_double, ctypes.c_int32,
                                        ctypes.c_int32, _vp, _vp, _vp, _vp]),
+    "mm_uneven_force_static": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(ctypes.c_int64),
+                                              ctypes.POINTER(UnevenOpts), _vp, _vp, ctypes.c_double,
+                                              ctypes.c_int32, _vp, _vp, _vp, _vp]),
     "mm_peak_probe": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int64, _dp, _dp, _vp]),
 }
 

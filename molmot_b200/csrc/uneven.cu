@@ -491,3 +491,129 @@ extern "C" int mm_uneven_force(const mm_uneven_plan *plan, const mm_beams *beams
     if (!rc) rc = launch_class<UC0>(P, plan, 0, persistent, st);
     return rc;
 }
+
+// ---------------------------------------------------------------------------
+// mm_uneven_force_static: mm_uneven_force without a plan and without any
+// allocation.  The work list and the three work counters live in a fixed
+// array in the module's device memory (one copy per GPU, held until the
+// process exits); the host side stages the work list in fixed host arrays.
+// Capacity: MM_STATIC_SCRATCH_BYTES = 1 MiB, i.e. kStaticMaxTasks = 43,680
+// work items (each covers chunk_groups x groups-per-CTA points).
+// Calls share that array and the host arrays: calls that overlap, from two
+// host threads or on two streams of one GPU, race.
+#define MM_STATIC_SCRATCH_BYTES (1u << 20)
+static __device__ __align__(256) unsigned char g_uneven_scratch[MM_STATIC_SCRATCH_BYTES];
+
+namespace {
+constexpr size_t kScratchHead = 256;  // int counters[3] at offset 0, work list from here
+constexpr int kStaticMaxTasks = (int)((MM_STATIC_SCRATCH_BYTES - kScratchHead) / sizeof(UnevenTask));
+constexpr int kMaxDevices = 64;
+UnevenTask h_st_tasks[kStaticMaxTasks];   // in creation order
+UnevenTask h_st_sorted[kStaticMaxTasks];  // in launch order
+double h_st_cost[kStaticMaxTasks];
+int h_st_order[kStaticMaxTasks];
+void *g_scratch_dev[kMaxDevices];         // address of g_uneven_scratch per device ordinal
+}  // namespace
+
+extern "C" int mm_uneven_force_static(const mm_bank *bank, const mm_beams *beams,
+                                      const int64_t *point_offsets, const mm_uneven_opts *opts,
+                                      const double *v, const double *z, double hbar,
+                                      int32_t uniform_fallback, double *F, double *R,
+                                      int32_t *status, void *stream)
+{
+    if (!bank || !beams || !point_offsets || !v || !z || !F) {
+        mm_set_error("bank, beams, point_offsets, v, z and F are required");
+        return -1;
+    }
+    const int n_mol = bank->n_mol;
+    if (beams->n_sets != n_mol) {
+        mm_set_error("beams must hold one parameter set per molecule (%d), got %d", n_mol, beams->n_sets);
+        return -1;
+    }
+    if (point_offsets[0] != 0) { mm_set_error("point_offsets[0] must be 0"); return -1; }
+    for (int m = 0; m < n_mol; m++)
+        if (point_offsets[m + 1] < point_offsets[m]) { mm_set_error("point_offsets must not decrease"); return -1; }
+    int dev = 0;
+    if (mm_cuda_check(cudaGetDevice(&dev), "cudaGetDevice")) return -3;
+    if (dev < 0 || dev >= kMaxDevices) { mm_set_error("device ordinal %d is above %d", dev, kMaxDevices - 1); return -1; }
+    if (!g_scratch_dev[dev]) {  // first call on this device
+        void *p = nullptr;
+        if (mm_cuda_check(cudaGetSymbolAddress(&p, g_uneven_scratch), "cudaGetSymbolAddress")) return -3;
+        g_scratch_dev[dev] = p;
+    }
+    mm_uneven_plan plan;  // a view of the fixed array; owns no memory
+    plan.bank = bank;
+    plan.n_mol = n_mol;
+    plan.n_points = point_offsets[n_mol];
+    const int G[3] = {16, 32, 32};
+    long long chunk[3];
+    const int chunk_groups = (opts && opts->chunk_groups > 0) ? opts->chunk_groups : 8;
+    for (int c = 0; c < 3; c++) {
+        int w = opts ? opts->warps_per_cta[c] : 0;
+        if (w <= 0) w = c == 0 ? 4 : 2;
+        if (w > 8) { mm_set_error("warps_per_cta must be <= 8"); return -1; }
+        plan.wpc[c] = w;
+        chunk[c] = (long long)(32 * w / G[c]) * chunk_groups;
+    }
+    long long n_items = 0;
+    for (int m = 0; m < n_mol; m++) {
+        const long long c = chunk[class_of(bank->ng[m], bank->ne[m])];
+        n_items += (point_offsets[m + 1] - point_offsets[m] + c - 1) / c;
+    }
+    if (n_items > kStaticMaxTasks) {
+        mm_set_error("mm_uneven_force_static: the batch makes %lld work items, above the %d that fit "
+                     "its fixed %u-byte scratch; raise chunk_groups, split the batch, or use "
+                     "mm_uneven_force", n_items, kStaticMaxTasks, (unsigned)MM_STATIC_SCRATCH_BYTES);
+        return -1;
+    }
+    if (plan.n_points == 0) return 0;
+    // work items of each class, largest cost first (ties in creation order, as
+    // the plan's stable sort); std::sort works in place
+    int base = 0;
+    for (int c = 0; c < 3; c++) {
+        int n = 0;
+        for (int m = 0; m < n_mol; m++) {
+            if (class_of(bank->ng[m], bank->ne[m]) != c) continue;
+            const double cost = (double)bank->ng[m] * bank->ng[m] * bank->ng[m] +
+                                8.0 * bank->ng[m] * bank->ne[m] * 8;
+            for (long long a = point_offsets[m]; a < point_offsets[m + 1]; a += chunk[c]) {
+                UnevenTask &t = h_st_tasks[base + n];
+                t.mol = m; t.pad = 0; t.p0 = a;
+                t.p1 = std::min<long long>(a + chunk[c], point_offsets[m + 1]);
+                h_st_cost[base + n] = cost * (double)(t.p1 - t.p0);
+                h_st_order[base + n] = base + n;
+                n++;
+            }
+        }
+        std::sort(h_st_order + base, h_st_order + base + n, [](int a, int b) {
+            return h_st_cost[a] > h_st_cost[b] || (h_st_cost[a] == h_st_cost[b] && a < b);
+        });
+        for (int i = base; i < base + n; i++) h_st_sorted[i] = h_st_tasks[h_st_order[i]];
+        plan.n_tasks[c] = n;
+        base += n;
+    }
+    unsigned char *scr = (unsigned char *)g_scratch_dev[dev];
+    UnevenTask *d_tasks = (UnevenTask *)(scr + kScratchHead);
+    for (int c = 0, b = 0; c < 3; b += plan.n_tasks[c], c++) plan.d_tasks[c] = d_tasks + b;
+    plan.d_counter = (int *)scr;
+    cudaStream_t st = (cudaStream_t)stream;
+    // the host arrays are pageable: the copy has taken them before it returns
+    if (mm_cuda_check(cudaMemcpyAsync(d_tasks, h_st_sorted, sizeof(UnevenTask) * base,
+                                      cudaMemcpyHostToDevice, st), "cudaMemcpyAsync"))
+        return -3;
+    // the work counters must start at zero on every call
+    if (mm_cuda_check(cudaMemsetAsync(plan.d_counter, 0, 3 * sizeof(int), st), "cudaMemsetAsync"))
+        return -3;
+    UnevenParams P;
+    P.ng = bank->d_ng; P.ne = bank->d_ne; P.off = bank->d_off; P.gam = bank->d_gam; P.kw = bank->d_k;
+    P.buf = bank->buf;
+    P.n_b = beams->n_b; P.kdir = beams->kdir; P.freq = beams->freq; P.s0 = beams->s0;
+    P.bgrad = beams->bgrad; P.pol = beams->pol; P.geff = beams->gamma_eff;
+    P.hbar = hbar > 0 ? hbar : MM_HBAR_JIT;
+    P.uniform_fb = uniform_fallback;
+    P.v = v; P.z = z; P.F = F; P.R = R; P.status = status;
+    int rc = launch_class<UC2>(P, &plan, 2, 1, st);
+    if (!rc) rc = launch_class<UC1>(P, &plan, 1, 1, st);
+    if (!rc) rc = launch_class<UC0>(P, &plan, 0, 1, st);
+    return rc;
+}

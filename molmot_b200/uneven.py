@@ -70,6 +70,7 @@ class UnevenBatch:
         self.bank, self.beams, self.hbar = bank, beams, hbar
         self.offsets = np.concatenate([[0], np.cumsum(np.asarray(point_counts, dtype=np.int64))])
         self.n_points = int(self.offsets[-1])
+        self._off_c = np.ascontiguousarray(self.offsets, dtype=np.int64)
         self.chunk_groups = chunk_groups
         self._plan(tuple(warps_per_cta))
 
@@ -105,6 +106,25 @@ class UnevenBatch:
                                          _dptr(out.get("R")), _dptr(out.get("status")),
                                          _stream_handle(stream))
         _lib.check(rc, "mm_uneven_force")
+        return out
+
+    def force_static(self, v, z, out, stream=None, uniform_fallback=False):
+        """The same forces through mm_uneven_force_static, which allocates
+        nothing: the caller passes `out` (F, and optionally R and status) and
+        the work list lives in the library's fixed device array.  Calls that
+        overlap in time race on that array."""
+        if v.numel() != self.n_points or z.numel() != self.n_points:
+            raise ValueError(f"expected {self.n_points} points")
+        o = _lib.UnevenOpts()
+        for i in range(3):
+            o.warps_per_cta[i] = int(self.wpc[i])
+        o.chunk_groups = int(self.chunk_groups)
+        rc = _lib.load().mm_uneven_force_static(
+            self.bank.handle, self.beams.handle,
+            self._off_c.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), ctypes.byref(o),
+            _dptr(v), _dptr(z), float(self.hbar), 1 if uniform_fallback else 0,
+            _dptr(out["F"]), _dptr(out.get("R")), _dptr(out.get("status")), _stream_handle(stream))
+        _lib.check(rc, "mm_uneven_force_static")
         return out
 
     def graph(self, v, z):
