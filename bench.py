@@ -8,15 +8,16 @@ v in [-10, 10] m/s and z in [-10, 10] mm: 2.68e8 steady-state force
 evaluations per step.  Synthetic inputs of exactly that shape (seed 20261203
 + rank).
 
-value      : force evaluations/s of the FP32-bulk + FP64-LU + refinement form,
+value      : force evaluations/s of the FP32-bulk form (FP32 Lorentzians, FP64
+             sums, populations from the FP64 solve of the excited-state chain),
              inputs resident, device-timed (CUDA events), max over ranks.
 plain_fp64 : the same for the plain FP64 form on the same grid.
 e2e        : the same metric through the public API with host arrays: per step
              the parameter sets and grid axes go host->device and the force
              map comes back device->host (inside the timed region).
 roofline   : the force kernel against the measured FP64/FP32 FMA peaks of
-             this GPU (mm_peak_probe); algorithmic FLOPs per point from
-             molmot_b200/flops.py.
+             this GPU (mm_peak_probe); algorithmic FLOPs per point of the form
+             that runs (molmot_b200/flops.py).
 cpu_baseline: the reference's numba core restated (oracle/rate_eq_numba.py)
              on all host cores, on a bounded sample of the same workload.
 
@@ -278,7 +279,7 @@ def main():
     import torch.distributed as dist
     from molmot_b200.molecules import load_sroh_from_julia
     from molmot_b200.engine import MoleculePack, BeamSets, force_batch
-    from molmot_b200.flops import active_triples, flops_per_point
+    from molmot_b200.flops import active_triples, flops_per_point, flops_reduced
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -378,7 +379,7 @@ def main():
                  if world == 1 and not args.no_secondary else None)
 
     A = active_triples(mol.d_squared, pol[0])
-    f64_32, f32_32 = flops_per_point(12, 4, 8, A, refine=True)
+    f64_32, f32_32 = flops_reduced(12, 4, A)
     f64_64, _ = flops_per_point(12, 4, 8, A, refine=False)
     # FP32 form: FP64 and FP32 pipes run concurrently; the bound is the slower of the two
     t_min32 = max(f64_32 * n_pts / (peaks["fp64"] * 1e12), f32_32 * n_pts / (peaks["fp32"] * 1e12))
@@ -400,7 +401,7 @@ def main():
             "data": "synthetic",
             "config": {"workload": f"SrOH (12 ground + 4 excited) batched force maps: {n_sets} "
                                    f"parameter sets x {NV}x{NZ} (v, z) grid per GPU, 8-beam DC MOT, "
-                                   "FP32 rates + FP64 LU + 1 refinement step",
+                                   "FP32 Lorentzians, FP64 sums, FP64 excited-chain population solve",
                        "points_per_step_per_gpu": n_pts, "parallelism": f"sets sharded, {world} GPU(s)",
                        "l2": "256 MB buffer written between timed steps (> 126 MB L2)"},
             "plain_fp64": {"value": total / (ms64 * 1e-3), "unit": "force evals/s",
@@ -412,7 +413,8 @@ def main():
                          "unit": "TFLOP/s", "frac": achieved32 / peak32, "traffic": None,
                          "peak_source": "mm_peak_probe FMA loop on this GPU: "
                                         f"fp64 {peaks['fp64']:.2f}, fp32 {peaks['fp32']:.2f} TFLOP/s",
-                         "flops_per_point": {"fp64": f64_32, "fp32": f32_32}},
+                         "flops_per_point": {"fp64": f64_32, "fp32": f32_32},
+                         "reference_algorithm_equivalent_tflops": f64_64 * n_pts / (ms32 * 1e-3) / 1e12},
             "e2e": {"value": total / (ms_e2e * 1e-3), "unit": "force evals/s",
                     "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                     "ms_per_step": ms_e2e},

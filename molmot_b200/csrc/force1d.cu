@@ -9,6 +9,7 @@
 #include <stdio.h>
 #include <algorithm>
 #include "rate_core.cuh"
+#include "reduced.cuh"
 
 namespace {
 
@@ -133,6 +134,57 @@ force_adjoint_kernel(ForceParams P, double *grad)
                 for (int i = t; i < 2 * nb; i += G) grad[gi * gw + i] = gacc[i];
             }
             __syncwarp();
+        }
+    }
+}
+
+// FP32-bulk form: one point per thread, populations from the reduced
+// (excited-manifold) solve of reduced.cuh.  One CTA per parameter set at a
+// time; its prologue builds the set's triple tables in shared memory, then the
+// threads stream over the set's points.
+#ifndef MM_RED_THREADS
+#define MM_RED_THREADS 128
+#endif
+#ifndef MM_RED_MINB
+#define MM_RED_MINB 5
+#endif
+constexpr int kRedThreads = MM_RED_THREADS;
+
+template <int NGMAX, int NEMAX, bool EXACT>
+__global__ void __launch_bounds__(kRedThreads, MM_RED_MINB)
+force_reduced_kernel(ForceParams P)
+{
+    extern __shared__ __align__(16) unsigned char sm[];
+    RedLayout<NGMAX, NEMAX> Ly;
+    Ly.build(P.n_b);
+    const long long pts_per_set = (P.layout == MM_LAYOUT_GRID) ? P.nv * P.nz : P.pps;
+    for (int set = blockIdx.y; set < P.n_sets; set += gridDim.y) {
+        const long long set_first = (long long)set * pts_per_set;
+        long long set_count = pts_per_set;
+        if (set_first + set_count > P.n_points) set_count = P.n_points - set_first;
+        if (set_count <= 0) continue;  // uniform over the CTA
+        RedView S;
+        __syncthreads();
+        build_reduced_tables<NGMAX, NEMAX>(P, set, sm, Ly, S);
+        const double Bg = P.bgrad[set];
+        const long long chunk = (set_count + gridDim.x - 1) / gridDim.x;
+        const long long start = (long long)blockIdx.x * chunk;
+        const long long end = min(start + chunk, set_count);
+        for (long long ip = start + threadIdx.x; ip < end; ip += blockDim.x) {
+            double v, z;
+            if (P.layout == MM_LAYOUT_GRID) {
+                v = P.v[ip / P.nz];
+                z = P.z[ip % P.nz];
+            } else {
+                v = P.v[set_first + ip];
+                z = P.z[set_first + ip];
+            }
+            const long long gi = set_first + ip;
+            double *pop = P.pop ? P.pop + gi * P.n_g : nullptr;
+            const RedOut o = reduced_point<NGMAX, NEMAX, EXACT>(P, S, v, z, Bg, pop);
+            P.F[gi] = o.F;
+            if (P.R) P.R[gi] = o.R;
+            if (P.status) P.status[gi] = o.status;
         }
     }
 }
@@ -294,6 +346,32 @@ int launch_force(const ForceParams &P, long long pts_per_set, cudaStream_t st)
 }
 
 template <class C>
+int launch_reduced(const ForceParams &P, long long pts_per_set, cudaStream_t st)
+{
+    auto kern = force_reduced_kernel<C::ng, C::ne, C::exact>;
+    RedLayout<C::ng, C::ne> Ly;
+    Ly.build(P.n_b);
+    const size_t sb = Ly.total;
+    if (sb > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb);
+        if (mm_cuda_check(e, "cudaFuncSetAttribute")) return -3;
+    }
+    int dev = 0, nsm = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kRedThreads, sb);
+    if (per_sm < 1) per_sm = 1;
+    // enough CTAs to fill the GPU a few times over, at least 8 points per thread
+    const long long want = (long long)nsm * per_sm * 4;
+    long long gx = std::max<long long>(1, want / std::max(1, P.n_sets));
+    gx = std::min(gx, std::max<long long>(1, (pts_per_set + kRedThreads * 8 - 1) / (kRedThreads * 8)));
+    gx = std::min<long long>(gx, 1 << 20);
+    dim3 grid((unsigned)gx, (unsigned)std::min(P.n_sets, 65535));
+    kern<<<grid, kRedThreads, sb, st>>>(P);
+    return mm_cuda_check(cudaGetLastError(), "force_reduced_kernel launch") ? -3 : 0;
+}
+
+template <class C>
 int launch_adjoint(const ForceParams &P, double *grad, cudaStream_t st)
 {
     auto kern = force_adjoint_kernel<C::ng, C::ne, C::g, C::exact>;
@@ -439,7 +517,7 @@ extern "C" int mm_force_batch(const mm_pack *pack, const mm_beams *beams, const 
     cudaStream_t st = (cudaStream_t)stream;
     return dispatch_class(P.n_g, P.n_e, [&](auto C) -> int {
         using CT = decltype(C);
-        return fp32 ? launch_force<CT, true>(P, pps, st) : launch_force<CT, false>(P, pps, st);
+        return fp32 ? launch_reduced<CT>(P, pps, st) : launch_force<CT, false>(P, pps, st);
     });
 }
 

@@ -1,0 +1,372 @@
+// reduced.cuh -- the FP32-bulk steady-state force, one point per thread,
+// with the population system solved exactly on the excited manifold.
+//
+// Model (molmot/obe/rate_equations_jit.py:18-145): rates R[g,e] (saturated),
+// r_g = sum_e R[g,e], M[g,k] = sum_e R[k,e] BR[e,g] - delta_gk r_k, the last
+// row replaced by ones, M' p = e_last, clamp, normalise, F = sum_g p_g F_g.
+//
+// Reduction.  Every column of M sums to zero (sum_g BR[e,g] = 1), so M' p =
+// e_last is M p = 0 with sum p = 1.  Row g of M p = 0 reads
+//     r_g p_g = sum_e BR[e,g] n_e,   n_e = sum_k R[k,e] p_k  (excitation flux),
+// hence p_g = (sum_e BR[e,g] n_e) / r_g and n = K n with the column-stochastic
+//     K[e,e'] = sum_g R[g,e] BR[e',g] / r_g   (n_e x n_e).
+// n is the stationary vector of the excited-state chain, computed by the
+// Grassmann-Taksar-Heyman state reduction (Gaussian elimination on I - K^T
+// written without subtractions, so every step adds non-negative numbers).
+// Then, with w_g = 1/r_g and phi_g = F_g / r_g,
+//     norm = sum_e n_e sum_g BR[e,g] w_g,   F = sum_e n_e sum_g BR[e,g] phi_g / norm,
+//     R    = sum_e n_e sum_g BR[e,g] / norm.
+// The per-ground-state sums are folded into K and two n_e-vectors while the
+// rates of g are computed, so a point keeps n_e^2 + 2 n_e FP64 accumulators.
+// The saturation factor 1/(1+s_g) cancels in R[g,e]/r_g and F_g/r_g and enters
+// only through w_g = (1+s_g)/sum_e R_unsat[g,e].
+//
+// Precision.  The Lorentzian of each (g, beam, e) triple runs in FP32 from
+// u = delta/(Gamma/2) = u0 + uv v - uB B (u0 rounded once from FP64); the
+// rate terms are summed in FP64 (the force sum cancels between
+// counter-propagating beams, and FP32 sums of those terms alone exceed 1e-6
+// of max|F| on some parameter sets).  Everything after the rates is FP64.
+//
+// Degenerate sets: a ground state with no active triple (r_g = 0), or an
+// excited-state chain that the state reduction cannot eliminate in index
+// order.  Both are properties of the parameter set (which triples exist), so
+// the CTA decides once per set and then solves every point with
+// dense_point(), the reference's own elimination in FP64 on the same rates.
+#pragma once
+#include "rate_core.cuh"
+
+// Unroll factor of the triple loop of one (ground, excited) pair.
+#ifndef MM_RED_UNROLL
+#define MM_RED_UNROLL 4
+#endif
+constexpr int kRedUnroll = MM_RED_UNROLL;
+
+// One active (ground g, beam b, excited e) triple: 32 bytes.
+struct TripR {
+    float u0;    // (freq_b - (E_e - E_g)) 2pi/(Gamma/2)  (FP64, rounded once)
+    float uv;    // (-k kdir_b / 2pi) 2pi/(Gamma/2)      per m/s
+    float uB;    // ((zd_e - zd_g) Gamma/2pi) 2pi/(Gamma/2) per G
+    float c1;    // (Gamma/2) s0_b d2 Geff
+    float c2;    // s0_b d2
+    int pad;
+    double hk;   // hbar k kdir_b
+};
+
+template <int NGMAX, int NEMAX>
+struct RedLayout {
+    // offs[g*NEMAX + e] .. offs[g*NEMAX + e + 1]: triples of (g, e), beams ascending
+    static constexpr int n_offs = NGMAX * NEMAX + 1;
+    size_t offs, brt, rsum, flags, trip, total;
+    __host__ __device__ static size_t al(size_t x) { return (x + 15) & ~size_t(15); }
+    __host__ __device__ void build(int n_b)
+    {
+        size_t o = 0;
+        offs = o;  o = al(o + sizeof(int) * n_offs);
+        brt = o;   o = al(o + sizeof(double) * NGMAX * NEMAX);   // BR[e,g] at [g][e]
+        rsum = o;  o = al(o + sizeof(double) * NEMAX);           // sum_g BR[e,g]
+        flags = o; o = al(o + sizeof(int) * 4);
+        trip = o;  o = al(o + sizeof(TripR) * (size_t)NGMAX * NEMAX * n_b);
+        total = o;
+    }
+};
+
+struct RedView {
+    const int *offs;
+    const double *brt, *rsum;
+    const TripR *trip;
+    int valid;
+};
+
+// Parameter-set tables for the reduced kernel (all threads of the CTA).
+template <int NGMAX, int NEMAX>
+__device__ void build_reduced_tables(const ForceParams &P, int set, unsigned char *sm,
+                                     const RedLayout<NGMAX, NEMAX> &Ly, RedView &S)
+{
+    const int n_g = P.n_g, n_e = P.n_e, n_b = P.n_b;
+    int *offs = (int *)(sm + Ly.offs), *flags = (int *)(sm + Ly.flags);
+    double *brt = (double *)(sm + Ly.brt), *rsum = (double *)(sm + Ly.rsum);
+    TripR *trip = (TripR *)(sm + Ly.trip);
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int32_t *pol = P.pol + (size_t)set * n_b;
+    const double *kdir = P.kdir + (size_t)set * n_b, *fr = P.freq + (size_t)set * n_b;
+    const double *s0 = P.s0 + (size_t)set * n_b;
+
+    // triple counts per (g, e) (d2 >= 1e-15, rate_equations_jit.py:67-69), BR transposed
+    for (int i = tid; i < NGMAX * NEMAX; i += nt) {
+        const int g = i / NEMAX, e = i % NEMAX;
+        int c = 0;
+        double br = 0.0;
+        if (g < n_g && e < n_e) {
+            for (int b = 0; b < n_b; b++)
+                if (P.d2[(g * n_e + e) * 3 + pol[b]] >= 1e-15) c++;
+            br = P.BR[e * n_g + g];
+        }
+        offs[i + 1] = c;
+        brt[i] = br;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        offs[0] = 0;
+        for (int i = 1; i <= NGMAX * NEMAX; i++) offs[i] += offs[i - 1];
+        // structural checks: every ground state pumped; excited chain reducible in index order
+        int valid = 1;
+        for (int g = 0; g < n_g; g++)
+            if (offs[g * NEMAX + NEMAX] == offs[g * NEMAX]) valid = 0;
+        bool T[NEMAX][NEMAX];  // T[i][j]: transition i -> j possible (decay to g, re-excitation to j)
+        for (int i = 0; i < NEMAX; i++)
+            for (int j = 0; j < NEMAX; j++) {
+                bool t = false;
+                if (i < n_e && j < n_e)
+                    for (int g = 0; g < n_g; g++)
+                        if (brt[g * NEMAX + i] > 0.0 && offs[g * NEMAX + j + 1] > offs[g * NEMAX + j]) t = true;
+                T[i][j] = t;
+            }
+        for (int k = n_e - 1; k >= 1; k--) {
+            bool s = false;
+            for (int j = 0; j < k; j++) s = s || T[k][j];
+            if (!s) valid = 0;
+            for (int i = 0; i < k; i++)
+                for (int j = 0; j < k; j++) T[i][j] = T[i][j] || (T[i][k] && T[k][j]);
+        }
+        for (int e = 0; e < NEMAX; e++) {
+            double a = 0.0;
+            for (int g = 0; g < n_g; g++) a += brt[g * NEMAX + e];
+            rsum[e] = a;
+        }
+        flags[0] = valid;
+    }
+    __syncthreads();
+    const double cu = MM_TWO_PI / (P.Gamma / 2.0);
+    const double gh = P.Gamma / 2.0;
+    for (int i = tid; i < NGMAX * NEMAX; i += nt) {
+        const int g = i / NEMAX, e = i % NEMAX;
+        if (g >= n_g || e >= n_e) continue;
+        int o = offs[i];
+        for (int b = 0; b < n_b; b++) {
+            const double d2 = P.d2[(g * n_e + e) * 3 + pol[b]];
+            if (d2 < 1e-15) continue;
+            TripR tr;
+            tr.u0 = (float)((fr[b] - (P.E[n_g + e] - P.E[g])) * cu);
+            tr.uv = (float)((-P.k * kdir[b]) / MM_TWO_PI * cu);
+            tr.uB = (float)((P.zd[n_g + e] - P.zd[g]) * P.Gamma / MM_TWO_PI * cu);
+            tr.c1 = (float)(gh * s0[b] * d2 * P.geff);
+            tr.c2 = (float)(s0[b] * d2);
+            tr.pad = 0;
+            tr.hk = P.hbar * P.k * kdir[b];
+            trip[o++] = tr;
+        }
+    }
+    __syncthreads();
+    S.offs = offs; S.brt = brt; S.rsum = rsum; S.trip = trip; S.valid = flags[0];
+}
+
+struct RedOut {
+    double F, R;
+    int status;
+};
+
+// Rates of ground state g at one point: unsaturated FP64 sums over the
+// triples of each excited state, the force sum, and the saturation sum.
+template <int NEMAX>
+__device__ __forceinline__ void reduced_rates(const RedView &S, int g, float vf, float Bf,
+                                              double (&Re)[NEMAX], double &f, float &s)
+{
+    f = 0.0;
+    s = 0.f;
+#pragma unroll
+    for (int e = 0; e < NEMAX; e++) {
+        double acc = 0.0;
+        const int i1 = S.offs[g * NEMAX + e + 1];
+#pragma unroll (kRedUnroll)
+        for (int i = S.offs[g * NEMAX + e]; i < i1; i++) {
+            const TripR tr = S.trip[i];
+            float u = fmaf(tr.uv, vf, tr.u0);
+            u = fmaf(-Bf, tr.uB, u);
+            const float L = mm_rcpf(fmaf(u, u, 1.0f));
+            const float ru = tr.c1 * L;
+            s = fmaf(tr.c2, L, s);
+            const double rd = (double)ru;
+            acc += rd;
+            f = fma(tr.hk, rd, f);
+        }
+        Re[e] = acc;
+    }
+}
+
+// Stationary vector of the column-stochastic K (K[to][from]) by state
+// reduction; returns false if a reduction step has no outflow.
+template <int NEMAX>
+__device__ __forceinline__ bool gth_stationary(double (&K)[NEMAX][NEMAX], int n_e, double (&pi)[NEMAX])
+{
+    bool ok = true;
+    // Q[i][j] = K[j][i]: probability i -> j
+#pragma unroll
+    for (int k = NEMAX - 1; k >= 1; k--) {
+        if (k < n_e) {
+            double S = 0.0;
+#pragma unroll
+            for (int j = 0; j < k; j++) S += K[j][k];
+            ok = ok && (S > 0.0);
+            const double inv = mm_rcp(S > 0.0 ? S : 1.0);
+#pragma unroll
+            for (int i = 0; i < k; i++) K[k][i] *= inv;            // Q[i][k] /= S
+#pragma unroll
+            for (int i = 0; i < k; i++)
+#pragma unroll
+                for (int j = 0; j < k; j++) K[j][i] = fma(K[k][i], K[j][k], K[j][i]);  // Q[i][j] += Q[i][k] Q[k][j]
+        }
+    }
+    pi[0] = 1.0;
+#pragma unroll
+    for (int k = 1; k < NEMAX; k++) {
+        double a = 0.0;
+        if (k < n_e) {
+#pragma unroll
+            for (int i = 0; i < k; i++) a = fma(pi[i], K[k][i], a);  // pi[i] Q[i][k]
+        }
+        pi[k] = a;
+    }
+    return ok;
+}
+
+// Dense fallback: the reference's elimination (rate_equations_jit.py:92-136)
+// in FP64 on the same FP32-bulk rates, one point per thread (local memory).
+template <int NGMAX, int NEMAX>
+__device__ __noinline__ RedOut dense_point(const ForceParams &P, const RedView &S, float vf, float Bf,
+                                           double *pop_out)
+{
+    const int n_g = P.n_g, n_e = P.n_e;
+    double R[NGMAX][NEMAX], Fk[NGMAX], Rk[NGMAX];
+    for (int g = 0; g < n_g; g++) {
+        double Re[NEMAX], f;
+        float s;
+        reduced_rates<NEMAX>(S, g, vf, Bf, Re, f, s);
+        const double sat = 1.0 / (1.0 + (double)s);
+        double rs = 0.0;
+        for (int e = 0; e < NEMAX; e++) { R[g][e] = Re[e] * sat; rs += R[g][e]; }
+        Rk[g] = rs;
+        Fk[g] = f * sat;
+    }
+    double A[NGMAX][NGMAX + 1];
+    for (int gg = 0; gg < n_g; gg++) {
+        for (int k = 0; k < n_g; k++) {
+            double a = (gg == k) ? -Rk[gg] : 0.0;
+            for (int e = 0; e < n_e; e++) a += R[k][e] * S.brt[gg * NEMAX + e];
+            A[gg][k] = a;
+        }
+        A[gg][n_g] = 0.0;
+    }
+    for (int k = 0; k < n_g; k++) A[n_g - 1][k] = 1.0;
+    A[n_g - 1][n_g] = 1.0;
+    int status = 0;
+    for (int col = 0; col < n_g; col++) {
+        int prow = col;
+        double mx = fabs(A[col][col]);
+        for (int r = col + 1; r < n_g; r++)
+            if (fabs(A[r][col]) > mx) { mx = fabs(A[r][col]); prow = r; }
+        if (prow != col)
+            for (int j = 0; j <= n_g; j++) { const double t = A[col][j]; A[col][j] = A[prow][j]; A[prow][j] = t; }
+        const double pv = A[col][col];
+        if (fabs(pv) < 1e-30) { status |= MM_ST_PIVOT; continue; }
+        for (int r = col + 1; r < n_g; r++) {
+            const double fct = A[r][col] / pv;
+            for (int j = col; j <= n_g; j++) A[r][j] -= fct * A[col][j];
+        }
+    }
+    double p[NGMAX];
+    for (int i = n_g - 1; i >= 0; i--) {
+        double sacc = A[i][n_g];
+        for (int j = i + 1; j < n_g; j++) sacc -= A[i][j] * p[j];
+        p[i] = (fabs(A[i][i]) > 1e-30) ? sacc / A[i][i] : 0.0;
+    }
+    double tot = 0.0;
+    for (int g = 0; g < n_g; g++) { if (p[g] < 0.0) p[g] = 0.0; tot += p[g]; }
+    if (tot > 0.0) {
+        for (int g = 0; g < n_g; g++) p[g] /= tot;
+    } else {
+        status |= MM_ST_ZERO_POP;
+        if (P.uniform_fb)
+            for (int g = 0; g < n_g; g++) p[g] = 1.0 / (double)n_g;
+    }
+    RedOut o;
+    o.F = 0.0;
+    o.R = 0.0;
+    for (int g = 0; g < n_g; g++) {
+        o.F += p[g] * Fk[g];
+        o.R += p[g] * Rk[g];
+        if (pop_out) pop_out[g] = p[g];
+    }
+    o.status = status;
+    return o;
+}
+
+// One point by the reduced solve.  pop_out (nullable): n_g populations.
+template <int NGMAX, int NEMAX, bool EXACT>
+__device__ __forceinline__ RedOut reduced_point(const ForceParams &P, const RedView &S, double v,
+                                                double z, double Bgrad, double *pop_out)
+{
+    const int n_g = EXACT ? NGMAX : P.n_g;
+    const int n_e = EXACT ? NEMAX : P.n_e;
+    const float vf = (float)v;
+    const float Bf = (float)__dmul_rn(__dmul_rn(Bgrad, z), 1e4);
+    if (!S.valid) return dense_point<NGMAX, NEMAX>(P, S, vf, Bf, pop_out);
+
+    double K[NEMAX][NEMAX], cw[NEMAX], cf[NEMAX];
+#pragma unroll
+    for (int e = 0; e < NEMAX; e++) {
+        cw[e] = 0.0;
+        cf[e] = 0.0;
+#pragma unroll
+        for (int e2 = 0; e2 < NEMAX; e2++) K[e][e2] = 0.0;
+    }
+    for (int g = 0; g < n_g; g++) {
+        double Re[NEMAX], f;
+        float s;
+        reduced_rates<NEMAX>(S, g, vf, Bf, Re, f, s);
+        double rt = 0.0;
+#pragma unroll
+        for (int e = 0; e < NEMAX; e++) rt += Re[e];
+        const double inv = mm_rcp(rt);             // rt > 0: every ground state is pumped
+        const double phi = f * inv;                // F_g / r_g
+        const double w = (1.0 + (double)s) * inv;  // 1 / r_g
+        double br[NEMAX];
+#pragma unroll
+        for (int e = 0; e < NEMAX; e++) br[e] = S.brt[g * NEMAX + e];
+#pragma unroll
+        for (int e = 0; e < NEMAX; e++) {
+            const double a = Re[e] * inv;          // R[g,e] / r_g
+#pragma unroll
+            for (int e2 = 0; e2 < NEMAX; e2++) K[e][e2] = fma(a, br[e2], K[e][e2]);
+        }
+#pragma unroll
+        for (int e = 0; e < NEMAX; e++) {
+            cw[e] = fma(br[e], w, cw[e]);
+            cf[e] = fma(br[e], phi, cf[e]);
+        }
+        if (pop_out) pop_out[g] = w;
+    }
+    double pi[NEMAX];
+    const bool ok = gth_stationary<NEMAX>(K, n_e, pi);
+    double nrm = 0.0, fn = 0.0, rn = 0.0;
+#pragma unroll
+    for (int e = 0; e < NEMAX; e++) {
+        nrm = fma(cw[e], pi[e], nrm);
+        fn = fma(cf[e], pi[e], fn);
+        rn = fma(S.rsum[e], pi[e], rn);
+    }
+    const double in = mm_rcp(nrm);
+    RedOut o;
+    o.F = fn * in;
+    o.R = rn * in;
+    o.status = 0;
+    if (pop_out) {
+        for (int g = 0; g < n_g; g++) {
+            double a = 0.0;
+#pragma unroll
+            for (int e = 0; e < NEMAX; e++) a = fma(S.brt[g * NEMAX + e], pi[e], a);
+            pop_out[g] = a * pop_out[g] * in;
+        }
+    }
+    if (!ok || !isfinite(o.F)) o.status |= MM_ST_NONFINITE;
+    return o;
+}

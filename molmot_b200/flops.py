@@ -38,3 +38,21 @@ def flops_per_point(n_g: int, n_e: int, n_b: int, A: int, refine: bool = False):
     fp32 = prelude + rates + sat
     fp64 = build + lu + back + tail + 3 * n_g * n_g
     return float(fp64), float(fp32)
+
+
+def flops_reduced(n_g: int, n_e: int, A: int):
+    """(fp64_flops, fp32_flops) of one point of the FP32-bulk form, which
+    solves the populations through the excited-state chain.
+
+    Per active triple: FP32 u = u0 + uv v - uB B (2 FMA), 1 + u^2 (1 FMA),
+    L = 1/(1 + u^2), rate = c1 L, s += c2 L (1 FMA): 10 FLOP; FP64 sums of the
+    rate and of hk * rate: 3 FLOP.  Per ground state (FP64): r_g, 1/r_g, F_g/r_g,
+    (1 + s_g)/r_g, R[g,e]/r_g, the K update (n_e^2 FMA) and two n_e-vector
+    updates.  The chain solve (state reduction of n_e states) and the final
+    three n_e dot products."""
+    fp32 = 10 * A
+    per_g = (n_e - 1) + 1 + 1 + 2 + n_e + 2 * n_e * n_e + 4 * n_e
+    gth = sum((k - 1) + 1 + k + 2 * k * k for k in range(1, n_e)) + sum(2 * k for k in range(1, n_e))
+    final = 3 * 2 * n_e + 3
+    fp64 = 3 * A + n_g * per_g + gth + final
+    return float(fp64), float(fp32)
