@@ -146,7 +146,7 @@ force_adjoint_kernel(ForceParams P, double *grad)
 #define MM_RED_THREADS 128
 #endif
 #ifndef MM_RED_MINB
-#define MM_RED_MINB 5
+#define MM_RED_MINB 4
 #endif
 constexpr int kRedThreads = MM_RED_THREADS;
 
@@ -181,7 +181,8 @@ force_reduced_kernel(ForceParams P)
             }
             const long long gi = set_first + ip;
             double *pop = P.pop ? P.pop + gi * P.n_g : nullptr;
-            const RedOut o = reduced_point<NGMAX, NEMAX, EXACT>(P, S, v, z, Bg, pop);
+            const RedOut o = (S.pad > 1) ? reduced_point<NGMAX, NEMAX, EXACT, kRedPad>(P, S, v, z, Bg, pop)
+                                         : reduced_point<NGMAX, NEMAX, EXACT, 1>(P, S, v, z, Bg, pop);
             P.F[gi] = o.F;
             if (P.R) P.R[gi] = o.R;
             if (P.status) P.status[gi] = o.status;

@@ -35,21 +35,20 @@
 #pragma once
 #include "rate_core.cuh"
 
-// Unroll factor of the triple loop of one (ground, excited) pair.
-#ifndef MM_RED_UNROLL
-#define MM_RED_UNROLL 4
-#endif
-constexpr int kRedUnroll = MM_RED_UNROLL;
+// Lists of the triples of one (ground, excited) pair may be padded with
+// zero-weight triples to a multiple of kRedPad, so the loop over a list runs
+// whole groups of kRedPad independent Lorentzians with no remainder.  A set
+// uses the padded lists when padding adds at most a quarter to its triples.
+constexpr int kRedPad = 4;
 
 // One active (ground g, beam b, excited e) triple: 32 bytes.
 struct TripR {
     float u0;    // (freq_b - (E_e - E_g)) 2pi/(Gamma/2)  (FP64, rounded once)
     float uv;    // (-k kdir_b / 2pi) 2pi/(Gamma/2)      per m/s
     float uB;    // ((zd_e - zd_g) Gamma/2pi) 2pi/(Gamma/2) per G
-    float c1;    // (Gamma/2) s0_b d2 Geff
     float c2;    // s0_b d2
-    int pad;
-    double hk;   // hbar k kdir_b
+    double c1;   // (Gamma/2) s0_b d2 Geff
+    double hc1;  // hbar k kdir_b c1
 };
 
 template <int NGMAX, int NEMAX>
@@ -65,7 +64,8 @@ struct RedLayout {
         brt = o;   o = al(o + sizeof(double) * NGMAX * NEMAX);   // BR[e,g] at [g][e]
         rsum = o;  o = al(o + sizeof(double) * NEMAX);           // sum_g BR[e,g]
         flags = o; o = al(o + sizeof(int) * 4);
-        trip = o;  o = al(o + sizeof(TripR) * (size_t)NGMAX * NEMAX * n_b);
+        trip = o;  o = al(o + sizeof(TripR) * (size_t)NGMAX * NEMAX *
+                                  (size_t)((n_b + kRedPad - 1) / kRedPad * kRedPad));
         total = o;
     }
 };
@@ -75,6 +75,7 @@ struct RedView {
     const double *brt, *rsum;
     const TripR *trip;
     int valid;
+    int pad;  // list granule: kRedPad or 1
 };
 
 // Parameter-set tables for the reduced kernel (all threads of the CTA).
@@ -106,8 +107,15 @@ __device__ void build_reduced_tables(const ForceParams &P, int set, unsigned cha
     }
     __syncthreads();
     if (tid == 0) {
+        int n_raw = 0, n_pad = 0;
+        for (int i = 1; i <= NGMAX * NEMAX; i++) {
+            n_raw += offs[i];
+            n_pad += (offs[i] + kRedPad - 1) / kRedPad * kRedPad;
+        }
+        const int pad = (4 * n_pad <= 5 * n_raw) ? kRedPad : 1;
+        flags[1] = pad;
         offs[0] = 0;
-        for (int i = 1; i <= NGMAX * NEMAX; i++) offs[i] += offs[i - 1];
+        for (int i = 1; i <= NGMAX * NEMAX; i++) offs[i] = offs[i - 1] + (offs[i] + pad - 1) / pad * pad;
         // structural checks: every ground state pumped; excited chain reducible in index order
         int valid = 1;
         for (int g = 0; g < n_g; g++)
@@ -149,15 +157,18 @@ __device__ void build_reduced_tables(const ForceParams &P, int set, unsigned cha
             tr.u0 = (float)((fr[b] - (P.E[n_g + e] - P.E[g])) * cu);
             tr.uv = (float)((-P.k * kdir[b]) / MM_TWO_PI * cu);
             tr.uB = (float)((P.zd[n_g + e] - P.zd[g]) * P.Gamma / MM_TWO_PI * cu);
-            tr.c1 = (float)(gh * s0[b] * d2 * P.geff);
             tr.c2 = (float)(s0[b] * d2);
-            tr.pad = 0;
-            tr.hk = P.hbar * P.k * kdir[b];
+            tr.c1 = gh * s0[b] * d2 * P.geff;
+            tr.hc1 = P.hbar * P.k * kdir[b] * tr.c1;
             trip[o++] = tr;
+        }
+        for (; o < offs[i + 1]; o++) {  // zero-weight padding: L = 1, every term 0
+            TripR tr = {};
+            trip[o] = tr;
         }
     }
     __syncthreads();
-    S.offs = offs; S.brt = brt; S.rsum = rsum; S.trip = trip; S.valid = flags[0];
+    S.offs = offs; S.brt = brt; S.rsum = rsum; S.trip = trip; S.valid = flags[0]; S.pad = flags[1];
 }
 
 struct RedOut {
@@ -165,9 +176,23 @@ struct RedOut {
     int status;
 };
 
+// One triple's Lorentzian (FP32) and its FP64 contributions.
+__device__ __forceinline__ void reduced_triple(const TripR &tr, float vf, float Bf, double &acc,
+                                               double &f, float &s)
+{
+    float u = fmaf(tr.uv, vf, tr.u0);
+    u = fmaf(-Bf, tr.uB, u);
+    const float L = mm_rcpf(fmaf(u, u, 1.0f));
+    s = fmaf(tr.c2, L, s);
+    const double Ld = (double)L;
+    acc = fma(tr.c1, Ld, acc);
+    f = fma(tr.hc1, Ld, f);
+}
+
 // Rates of ground state g at one point: unsaturated FP64 sums over the
 // triples of each excited state, the force sum, and the saturation sum.
-template <int NEMAX>
+// PAD: the set's list granule (kRedPad or 1).
+template <int NEMAX, int PAD>
 __device__ __forceinline__ void reduced_rates(const RedView &S, int g, float vf, float Bf,
                                               double (&Re)[NEMAX], double &f, float &s)
 {
@@ -177,17 +202,15 @@ __device__ __forceinline__ void reduced_rates(const RedView &S, int g, float vf,
     for (int e = 0; e < NEMAX; e++) {
         double acc = 0.0;
         const int i1 = S.offs[g * NEMAX + e + 1];
-#pragma unroll (kRedUnroll)
-        for (int i = S.offs[g * NEMAX + e]; i < i1; i++) {
-            const TripR tr = S.trip[i];
-            float u = fmaf(tr.uv, vf, tr.u0);
-            u = fmaf(-Bf, tr.uB, u);
-            const float L = mm_rcpf(fmaf(u, u, 1.0f));
-            const float ru = tr.c1 * L;
-            s = fmaf(tr.c2, L, s);
-            const double rd = (double)ru;
-            acc += rd;
-            f = fma(tr.hk, rd, f);
+        if constexpr (PAD > 1) {
+#pragma unroll 1
+            for (int i = S.offs[g * NEMAX + e]; i < i1; i += PAD) {
+#pragma unroll
+                for (int j = 0; j < PAD; j++) reduced_triple(S.trip[i + j], vf, Bf, acc, f, s);
+            }
+        } else {
+#pragma unroll 4
+            for (int i = S.offs[g * NEMAX + e]; i < i1; i++) reduced_triple(S.trip[i], vf, Bf, acc, f, s);
         }
         Re[e] = acc;
     }
@@ -240,7 +263,8 @@ __device__ __noinline__ RedOut dense_point(const ForceParams &P, const RedView &
     for (int g = 0; g < n_g; g++) {
         double Re[NEMAX], f;
         float s;
-        reduced_rates<NEMAX>(S, g, vf, Bf, Re, f, s);
+        if (S.pad > 1) reduced_rates<NEMAX, kRedPad>(S, g, vf, Bf, Re, f, s);
+        else reduced_rates<NEMAX, 1>(S, g, vf, Bf, Re, f, s);
         const double sat = 1.0 / (1.0 + (double)s);
         double rs = 0.0;
         for (int e = 0; e < NEMAX; e++) { R[g][e] = Re[e] * sat; rs += R[g][e]; }
@@ -301,7 +325,7 @@ __device__ __noinline__ RedOut dense_point(const ForceParams &P, const RedView &
 }
 
 // One point by the reduced solve.  pop_out (nullable): n_g populations.
-template <int NGMAX, int NEMAX, bool EXACT>
+template <int NGMAX, int NEMAX, bool EXACT, int PAD>
 __device__ __forceinline__ RedOut reduced_point(const ForceParams &P, const RedView &S, double v,
                                                 double z, double Bgrad, double *pop_out)
 {
@@ -322,7 +346,7 @@ __device__ __forceinline__ RedOut reduced_point(const ForceParams &P, const RedV
     for (int g = 0; g < n_g; g++) {
         double Re[NEMAX], f;
         float s;
-        reduced_rates<NEMAX>(S, g, vf, Bf, Re, f, s);
+        reduced_rates<NEMAX, PAD>(S, g, vf, Bf, Re, f, s);
         double rt = 0.0;
 #pragma unroll
         for (int e = 0; e < NEMAX; e++) rt += Re[e];
