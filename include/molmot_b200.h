@@ -38,7 +38,9 @@ extern "C" {
 
 /* precision of the force kernels */
 #define MM_PREC_FP64 0         /* plain FP64, reference operation order */
-#define MM_PREC_FP32_REFINE 1  /* FP32 rates/shifts/reductions, FP64 LU + 1 refinement step */
+#define MM_PREC_FP32_REFINE 1  /* FP32-bulk: FP32 Lorentzians with FP64 sums; force batches solve
+                                  the populations in FP64 through the excited-state chain
+                                  (reduced.cuh), trajectories by FP64 LU + 1 refinement step */
 
 /* point layouts of mm_force_batch */
 #define MM_LAYOUT_POINTS 0 /* v[i], z[i]; point i belongs to set i / points_per_set */
@@ -108,6 +110,13 @@ MM_API int mm_pack_destroy(mm_pack *pack);
  * (molmot_cuda/rate_equations_cuda.py:370-397, 427-441). */
 MM_API int mm_beams_create(const mm_beam_desc *desc, int32_t n_sets, mm_beams **out);
 MM_API int mm_beams_destroy(mm_beams *beams);
+
+/* A handle for the parameter sets [first_set, first_set + n_sets) of `parent`
+ * that shares the parent's device arrays (no device allocation or copy), so a
+ * long batch can be computed in chunks, e.g. to overlap each chunk's
+ * device->host copy with the next chunk's computation.  No counterpart in the
+ * reference.  Destroy it with mm_beams_destroy before the parent. */
+MM_API int mm_beams_view(const mm_beams *parent, int32_t first_set, int32_t n_sets, mm_beams **out);
 
 /*
  * Steady-state force, populations and scattering rate for a batch of points.

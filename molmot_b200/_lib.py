@@ -83,6 +83,7 @@ SIGNATURES = {
                                      ctypes.c_int64, ctypes.c_double, ctypes.c_double,
                                      ctypes.c_int32, ctypes.c_uint64, ctypes.c_double,
                                      _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "mm_beams_view": (ctypes.c_int, [_vp, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(_vp)]),
     "mm_bank_create": (ctypes.c_int, [ctypes.POINTER(MolDesc), ctypes.c_int32, ctypes.POINTER(_vp)]),
     "mm_bank_destroy": (ctypes.c_int, [_vp]),
     "mm_uneven_plan_create": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int64),

@@ -159,8 +159,31 @@ extern "C" int mm_beams_create(const mm_beam_desc *d, int32_t n_sets, mm_beams *
 extern "C" int mm_beams_destroy(mm_beams *b)
 {
     if (!b) return 0;
-    cudaFree(b->kdir); cudaFree(b->freq); cudaFree(b->s0); cudaFree(b->pol);
-    cudaFree(b->bgrad); cudaFree(b->khat); cudaFree(b->radius);
+    if (!b->view) {
+        cudaFree(b->kdir); cudaFree(b->freq); cudaFree(b->s0); cudaFree(b->pol);
+        cudaFree(b->bgrad); cudaFree(b->khat); cudaFree(b->radius);
+    }
     delete b;
+    return 0;
+}
+
+extern "C" int mm_beams_view(const mm_beams *parent, int32_t first_set, int32_t n_sets, mm_beams **out)
+{
+    if (!out) { mm_set_error("out is null"); return -1; }
+    *out = nullptr;
+    if (!parent) { mm_set_error("parent is null"); return -1; }
+    if (first_set < 0 || n_sets < 1 || first_set + (long long)n_sets > parent->n_sets) {
+        mm_set_error("sets [%d, %d) outside the parent's %d", first_set, first_set + n_sets, parent->n_sets);
+        return -1;
+    }
+    mm_beams *b = new mm_beams(*parent);
+    const size_t o = (size_t)first_set * parent->n_b;
+    b->n_sets = n_sets;
+    b->kdir += o; b->freq += o; b->s0 += o; b->pol += o;
+    b->bgrad += first_set;
+    if (b->khat) b->khat += 3 * o;
+    if (b->radius) b->radius += o;
+    b->view = 1;
+    *out = b;
     return 0;
 }

@@ -42,6 +42,7 @@ struct mm_beams {
     int device;
     double *kdir, *freq, *s0, *bgrad, *khat, *radius;  // device
     int32_t *pol;                                       // device
+    int view;  // 1: the arrays belong to another handle (mm_beams_view)
 };
 
 // Parameters of the 1D force kernels (passed by value).

@@ -147,6 +147,18 @@ class BeamSets:
         s0 = [[b.s0 for b in L] for L in beam_lists]
         return cls(kdir, freq, pol, s0, b_gradient, gamma_eff)
 
+    def view(self, first_set: int, n_sets: int) -> "BeamSets":
+        """Sets [first_set, first_set + n_sets) as a handle sharing this one's
+        device arrays (mm_beams_view; no device allocation or copy)."""
+        h = ctypes.c_void_p()
+        _lib.check(_lib.load().mm_beams_view(self.handle, int(first_set), int(n_sets), ctypes.byref(h)),
+                   "mm_beams_view")
+        v = BeamSets.__new__(BeamSets)
+        v.n_sets, v.n_beams, v.gamma_eff = int(n_sets), self.n_beams, self.gamma_eff
+        v._keep = [self]  # the parent's arrays must outlive the view
+        v.handle = h
+        return v
+
     def __del__(self):
         h = getattr(self, "handle", None)
         if h is not None and h.value:
@@ -209,6 +221,60 @@ def force_batch(pack: MoleculePack, beams: BeamSets, v, z, *, grid: bool = False
                                     _dptr(out.get("pop")), _dptr(out.get("status")),
                                     _stream_handle(stream))
     _lib.check(rc, "mm_force_batch")
+    return out
+
+
+_COPY_STREAMS = {}
+
+
+def force_maps_to_host(pack: MoleculePack, beams: BeamSets, v, z, out=None, *, precision="fp32",
+                       hbar=None, chunk_sets: int = 256, sync: bool = True):
+    """Force maps F[n_sets, nv, nz] of every parameter set (grid layout) in
+    host memory.
+
+    The sets are computed in chunks of ``chunk_sets`` on the current stream,
+    alternating between two device buffers; each chunk's device->host copy runs
+    on a second stream while the next chunk is computed, so the transfer of
+    the maps hides the computation.  ``out``: a host float64 tensor of that
+    shape (page-locked for overlapped copies; allocated page-locked if None).
+    With sync=False the call returns once everything is enqueued and the maps
+    are complete when the current stream reaches that point.
+    """
+    v = _to_dev(v)
+    z = _to_dev(z)
+    dev = v.device
+    nv, nz, n_sets = v.numel(), z.numel(), beams.n_sets
+    if out is None:
+        out = torch.empty((n_sets, nv, nz), dtype=torch.float64, pin_memory=True)
+    if tuple(out.shape) != (n_sets, nv, nz) or out.dtype != torch.float64 or out.is_cuda:
+        raise ValueError(f"out must be a host float64 tensor of shape {(n_sets, nv, nz)}")
+    chunk = max(1, min(int(chunk_sets), n_sets))
+    comp = torch.cuda.current_stream(dev)
+    copy = _COPY_STREAMS.get(dev.index)
+    if copy is None:
+        copy = _COPY_STREAMS[dev.index] = torch.cuda.Stream(device=dev)
+    bufs = [torch.empty((chunk, nv, nz), dtype=torch.float64, device=dev) for _ in range(2)]
+    free = [None, None]  # event: the copy out of buffer b has finished
+    for i, first in enumerate(range(0, n_sets, chunk)):
+        n = min(chunk, n_sets - first)
+        b = i % 2
+        if free[b] is not None:
+            comp.wait_event(free[b])
+        force_batch(pack, beams.view(first, n), v, z, grid=True, precision=precision, hbar=hbar,
+                    want_pop=False, want_R=False, want_status=False, out={"F": bufs[b][:n]},
+                    stream=comp)
+        done = torch.cuda.Event()
+        done.record(comp)
+        copy.wait_event(done)
+        with torch.cuda.stream(copy):
+            out[first:first + n].copy_(bufs[b][:n], non_blocking=True)
+        free[b] = torch.cuda.Event()
+        free[b].record(copy)
+    for t in bufs:
+        t.record_stream(copy)
+    comp.wait_stream(copy)
+    if sync:
+        comp.synchronize()
     return out
 
 

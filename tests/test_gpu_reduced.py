@@ -102,3 +102,22 @@ def test_fp32_form_equals_between_layouts(mol, pack):
     zp = np.tile(Z.ravel(), 3)
     b = force_batch(pack, bs, vp, zp, points_per_set=V.size, precision="fp32")["F"].cpu().numpy()
     assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("precision,chunk", [("fp32", 2), ("fp64", 3), ("fp32", 64)])
+def test_force_maps_to_host_chunks_equal_one_launch(mol, pack, precision, chunk):
+    """Chunked computation with overlapped device->host copies (beam-set views)
+    gives the same maps bit for bit as one launch over all sets."""
+    import bench
+    import torch
+    from molmot_b200.engine import BeamSets, force_batch, force_maps_to_host
+    kdir, freq, pol, s0, B = bench.make_params(mol, 7, 5)
+    bs = BeamSets(kdir, freq, pol, s0, B)
+    v = np.linspace(-10, 10, 19)
+    z = np.linspace(-1e-2, 1e-2, 23)
+    ref = force_batch(pack, bs, v, z, grid=True, precision=precision)["F"].cpu()
+    host = force_maps_to_host(pack, bs, v, z, precision=precision, chunk_sets=chunk)
+    assert not host.is_cuda and host.is_pinned()
+    assert torch.equal(host, ref)
+    with pytest.raises(RuntimeError):
+        bs.view(5, 3)  # beyond the parent's 7 sets
