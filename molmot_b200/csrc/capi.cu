@@ -103,6 +103,8 @@ extern "C" int mm_pack_create(const mm_mol_desc *d, mm_pack **out)
     }
     for (size_t i = 0; i < o; i++)
         if (!isfinite(h[i])) { mm_set_error("molecule data contains a non-finite value"); delete p; return -1; }
+    p->act.resize((size_t)n_g * n_e * 3);
+    for (size_t i = 0; i < p->act.size(); i++) p->act[i] = d->d_squared[i] >= 1e-15 ? 1 : 0;
     if (upload(&p->buf, h.data(), o)) { delete p; return -3; }
     *out = p;
     return 0;
@@ -141,6 +143,8 @@ extern "C" int mm_beams_create(const mm_beam_desc *d, int32_t n_sets, mm_beams *
         if (!isfinite(d->b_gradient[s])) { mm_set_error("set %d has a non-finite B gradient", s); return -1; }
     mm_beams *b = new mm_beams();
     b->n_sets = n_sets; b->n_b = n_b; b->gamma_eff = d->gamma_eff;
+    b->h_pol_store = std::make_shared<std::vector<int32_t>>(d->pol, d->pol + nb);
+    b->h_pol = b->h_pol_store->data();
     b->has3d = (d->khat != nullptr) ? 1 : 0;
     cudaGetDevice(&b->device);
     int rc = 0;
@@ -180,6 +184,7 @@ extern "C" int mm_beams_view(const mm_beams *parent, int32_t first_set, int32_t 
     const size_t o = (size_t)first_set * parent->n_b;
     b->n_sets = n_sets;
     b->kdir += o; b->freq += o; b->s0 += o; b->pol += o;
+    b->h_pol += o;
     b->bgrad += first_set;
     if (b->khat) b->khat += 3 * o;
     if (b->radius) b->radius += o;

@@ -3,6 +3,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <math.h>
+#include <memory>
+#include <vector>
 
 #include "../../include/molmot_b200.h"
 
@@ -32,6 +34,7 @@ struct mm_pack {
     size_t n_buf;    // doubles
     // offsets (in doubles) into buf
     size_t oE, ozd, od2, oBR, oZre, oZim, oZe, oTdm;
+    std::vector<unsigned char> act;  // host: d2[g][e][q] >= 1e-15 (active triple pattern)
 };
 
 // Device-resident parameter sets of beams.
@@ -43,6 +46,8 @@ struct mm_beams {
     double *kdir, *freq, *s0, *bgrad, *khat, *radius;  // device
     int32_t *pol;                                       // device
     int view;  // 1: the arrays belong to another handle (mm_beams_view)
+    std::shared_ptr<std::vector<int32_t>> h_pol_store;  // host copy of pol (shared by views)
+    const int32_t *h_pol;                               // this handle's first set in it
 };
 
 // Parameters of the 1D force kernels (passed by value).

@@ -148,9 +148,10 @@ force_adjoint_kernel(ForceParams P, double *grad)
 #ifndef MM_RED_MINB
 #define MM_RED_MINB 4
 #endif
+
 constexpr int kRedThreads = MM_RED_THREADS;
 
-template <int NGMAX, int NEMAX, bool EXACT>
+template <int NGMAX, int NEMAX, bool EXACT, int PAD>
 __global__ void __launch_bounds__(kRedThreads, MM_RED_MINB)
 force_reduced_kernel(ForceParams P)
 {
@@ -165,14 +166,20 @@ force_reduced_kernel(ForceParams P)
         if (set_count <= 0) continue;  // uniform over the CTA
         RedView S;
         __syncthreads();
-        build_reduced_tables<NGMAX, NEMAX>(P, set, sm, Ly, S);
+        build_reduced_tables<NGMAX, NEMAX, PAD>(P, set, sm, Ly, S);
         const double Bg = P.bgrad[set];
         const long long chunk = (set_count + gridDim.x - 1) / gridDim.x;
         const long long start = (long long)blockIdx.x * chunk;
         const long long end = min(start + chunk, set_count);
+        const bool idx32 = P.layout == MM_LAYOUT_GRID && end <= 0x7fffffffll;
         for (long long ip = start + threadIdx.x; ip < end; ip += blockDim.x) {
             double v, z;
-            if (P.layout == MM_LAYOUT_GRID) {
+            if (idx32) {  // 32-bit division for grids below 2^31 points per set
+                const unsigned iu = (unsigned)ip, nz = (unsigned)P.nz;
+                const unsigned iv = iu / nz;
+                v = P.v[iv];
+                z = P.z[iu - iv * nz];
+            } else if (P.layout == MM_LAYOUT_GRID) {
                 v = P.v[ip / P.nz];
                 z = P.z[ip % P.nz];
             } else {
@@ -181,8 +188,7 @@ force_reduced_kernel(ForceParams P)
             }
             const long long gi = set_first + ip;
             double *pop = P.pop ? P.pop + gi * P.n_g : nullptr;
-            const RedOut o = (S.pad > 1) ? reduced_point<NGMAX, NEMAX, EXACT, kRedPad>(P, S, v, z, Bg, pop)
-                                         : reduced_point<NGMAX, NEMAX, EXACT, 1>(P, S, v, z, Bg, pop);
+            const RedOut o = reduced_point<NGMAX, NEMAX, EXACT, PAD>(P, S, v, z, Bg, pop);
             P.F[gi] = o.F;
             if (P.R) P.R[gi] = o.R;
             if (P.status) P.status[gi] = o.status;
@@ -346,10 +352,10 @@ int launch_force(const ForceParams &P, long long pts_per_set, cudaStream_t st)
     return mm_cuda_check(cudaGetLastError(), "force_kernel launch") ? -3 : 0;
 }
 
-template <class C>
+template <class C, int PAD>
 int launch_reduced(const ForceParams &P, long long pts_per_set, cudaStream_t st)
 {
-    auto kern = force_reduced_kernel<C::ng, C::ne, C::exact>;
+    auto kern = force_reduced_kernel<C::ng, C::ne, C::exact, PAD>;
     RedLayout<C::ng, C::ne> Ly;
     Ly.build(P.n_b);
     const size_t sb = Ly.total;
@@ -409,6 +415,28 @@ int launch_traj(const ForceParams &P, const TrajParams &T, cudaStream_t st)
     const long long gx = (T.n_particles + ngroups - 1) / ngroups;
     kern<<<(unsigned)gx, kThreads, sb, st>>>(P, T);
     return mm_cuda_check(cudaGetLastError(), "traj1d_kernel launch") ? -3 : 0;
+}
+
+// List granule of the reduced kernel for a batch: kRedPad when padding every
+// (ground, excited) triple list to a multiple of kRedPad adds at most a quarter
+// to the batch's triples, else 1.  The triple count of a pair is
+// sum_q active[g][e][q] * (beams of the set with polarisation q), from the
+// host copies kept in the handles.
+int reduced_list_granule(const mm_pack *pack, const mm_beams *beams)
+{
+    const int n_g = pack->n_g, n_e = pack->n_e, n_b = beams->n_b;
+    long long n_raw = 0, n_pad = 0;
+    for (int s = 0; s < beams->n_sets; s++) {
+        int npol[3] = {0, 0, 0};
+        for (int b = 0; b < n_b; b++) npol[beams->h_pol[(size_t)s * n_b + b]]++;
+        for (int i = 0; i < n_g * n_e; i++) {
+            const unsigned char *a = &pack->act[(size_t)i * 3];
+            const int c = a[0] * npol[0] + a[1] * npol[1] + a[2] * npol[2];
+            n_raw += c;
+            n_pad += (c + kRedPad - 1) / kRedPad * kRedPad;
+        }
+    }
+    return (4 * n_pad <= 5 * n_raw) ? kRedPad : 1;
 }
 
 // Size-class dispatch.  SrOH (12 ground, 4 excited) has an exact class.
@@ -518,7 +546,9 @@ extern "C" int mm_force_batch(const mm_pack *pack, const mm_beams *beams, const 
     cudaStream_t st = (cudaStream_t)stream;
     return dispatch_class(P.n_g, P.n_e, [&](auto C) -> int {
         using CT = decltype(C);
-        return fp32 ? launch_reduced<CT>(P, pps, st) : launch_force<CT, false>(P, pps, st);
+        if (!fp32) return launch_force<CT, false>(P, pps, st);
+        return reduced_list_granule(pack, beams) == kRedPad ? launch_reduced<CT, kRedPad>(P, pps, st)
+                                                            : launch_reduced<CT, 1>(P, pps, st);
     });
 }
 

@@ -37,8 +37,10 @@
 
 // Lists of the triples of one (ground, excited) pair may be padded with
 // zero-weight triples to a multiple of kRedPad, so the loop over a list runs
-// whole groups of kRedPad independent Lorentzians with no remainder.  A set
-// uses the padded lists when padding adds at most a quarter to its triples.
+// whole groups of kRedPad independent Lorentzians with no remainder.  The
+// host picks the granule per launch (kRedPad when padding adds at most a
+// quarter to the batch's triples, else 1); it is a template parameter of
+// the kernel, which then holds one loop form only.
 constexpr int kRedPad = 4;
 
 // One active (ground g, beam b, excited e) triple: 32 bytes.
@@ -75,11 +77,11 @@ struct RedView {
     const double *brt, *rsum;
     const TripR *trip;
     int valid;
-    int pad;  // list granule: kRedPad or 1
 };
 
-// Parameter-set tables for the reduced kernel (all threads of the CTA).
-template <int NGMAX, int NEMAX>
+// Parameter-set tables for the reduced kernel (all threads of the CTA);
+// lists padded to multiples of PAD.
+template <int NGMAX, int NEMAX, int PAD>
 __device__ void build_reduced_tables(const ForceParams &P, int set, unsigned char *sm,
                                      const RedLayout<NGMAX, NEMAX> &Ly, RedView &S)
 {
@@ -107,15 +109,8 @@ __device__ void build_reduced_tables(const ForceParams &P, int set, unsigned cha
     }
     __syncthreads();
     if (tid == 0) {
-        int n_raw = 0, n_pad = 0;
-        for (int i = 1; i <= NGMAX * NEMAX; i++) {
-            n_raw += offs[i];
-            n_pad += (offs[i] + kRedPad - 1) / kRedPad * kRedPad;
-        }
-        const int pad = (4 * n_pad <= 5 * n_raw) ? kRedPad : 1;
-        flags[1] = pad;
         offs[0] = 0;
-        for (int i = 1; i <= NGMAX * NEMAX; i++) offs[i] = offs[i - 1] + (offs[i] + pad - 1) / pad * pad;
+        for (int i = 1; i <= NGMAX * NEMAX; i++) offs[i] = offs[i - 1] + (offs[i] + PAD - 1) / PAD * PAD;
         // structural checks: every ground state pumped; excited chain reducible in index order
         int valid = 1;
         for (int g = 0; g < n_g; g++)
@@ -168,7 +163,7 @@ __device__ void build_reduced_tables(const ForceParams &P, int set, unsigned cha
         }
     }
     __syncthreads();
-    S.offs = offs; S.brt = brt; S.rsum = rsum; S.trip = trip; S.valid = flags[0]; S.pad = flags[1];
+    S.offs = offs; S.brt = brt; S.rsum = rsum; S.trip = trip; S.valid = flags[0];
 }
 
 struct RedOut {
@@ -191,7 +186,7 @@ __device__ __forceinline__ void reduced_triple(const TripR &tr, float vf, float 
 
 // Rates of ground state g at one point: unsaturated FP64 sums over the
 // triples of each excited state, the force sum, and the saturation sum.
-// PAD: the set's list granule (kRedPad or 1).
+// PAD: the list granule (kRedPad or 1).
 template <int NEMAX, int PAD>
 __device__ __forceinline__ void reduced_rates(const RedView &S, int g, float vf, float Bf,
                                               double (&Re)[NEMAX], double &f, float &s)
@@ -254,7 +249,7 @@ __device__ __forceinline__ bool gth_stationary(double (&K)[NEMAX][NEMAX], int n_
 
 // Dense fallback: the reference's elimination (rate_equations_jit.py:92-136)
 // in FP64 on the same FP32-bulk rates, one point per thread (local memory).
-template <int NGMAX, int NEMAX>
+template <int NGMAX, int NEMAX, int PAD>
 __device__ __noinline__ RedOut dense_point(const ForceParams &P, const RedView &S, float vf, float Bf,
                                            double *pop_out)
 {
@@ -263,8 +258,7 @@ __device__ __noinline__ RedOut dense_point(const ForceParams &P, const RedView &
     for (int g = 0; g < n_g; g++) {
         double Re[NEMAX], f;
         float s;
-        if (S.pad > 1) reduced_rates<NEMAX, kRedPad>(S, g, vf, Bf, Re, f, s);
-        else reduced_rates<NEMAX, 1>(S, g, vf, Bf, Re, f, s);
+        reduced_rates<NEMAX, PAD>(S, g, vf, Bf, Re, f, s);
         const double sat = 1.0 / (1.0 + (double)s);
         double rs = 0.0;
         for (int e = 0; e < NEMAX; e++) { R[g][e] = Re[e] * sat; rs += R[g][e]; }
@@ -333,7 +327,15 @@ __device__ __forceinline__ RedOut reduced_point(const ForceParams &P, const RedV
     const int n_e = EXACT ? NEMAX : P.n_e;
     const float vf = (float)v;
     const float Bf = (float)__dmul_rn(__dmul_rn(Bgrad, z), 1e4);
-    if (!S.valid) return dense_point<NGMAX, NEMAX>(P, S, vf, Bf, pop_out);
+    if (!(isfinite(v) && isfinite(z))) {  // the rate chain assumes finite, normal Lorentzians
+        RedOut o;
+        o.F = o.R = __longlong_as_double(0x7ff8000000000000ll);
+        o.status = MM_ST_NONFINITE;
+        if (pop_out)
+            for (int g = 0; g < n_g; g++) pop_out[g] = o.F;
+        return o;
+    }
+    if (!S.valid) return dense_point<NGMAX, NEMAX, PAD>(P, S, vf, Bf, pop_out);
 
     double K[NEMAX][NEMAX], cw[NEMAX], cf[NEMAX];
 #pragma unroll

@@ -121,3 +121,25 @@ def test_force_maps_to_host_chunks_equal_one_launch(mol, pack, precision, chunk)
     assert torch.equal(host, ref)
     with pytest.raises(RuntimeError):
         bs.view(5, 3)  # beyond the parent's 7 sets
+
+
+def test_list_granules_agree(mol, pack):
+    """The host pads triple lists to groups of 4 when that adds at most a
+    quarter to the batch's triples.  A set whose own lists are ragged (8 beams
+    with polarisations sigma+, sigma-, pi mixed) gets granule 1 alone and
+    granule 4 inside a batch of bench-pattern sets; zero-weight padding adds
+    exact zeros, so both give the same maps bit for bit, and both match the
+    oracle."""
+    import bench
+    from molmot_b200.engine import BeamSets, force_batch
+    kdir, freq, pol, s0, B = bench.make_params(mol, 16, 11)
+    pol[0] = [2, 0, 1, 2, 0, 1, 2, 0]
+    v = np.linspace(-10, 10, 21)
+    z = np.linspace(-1e-2, 1e-2, 17)
+    alone = force_batch(pack, BeamSets(kdir[:1], freq[:1], pol[:1], s0[:1], B[:1]), v, z, grid=True,
+                        precision="fp32")["F"].cpu().numpy()[0]
+    batch = force_batch(pack, BeamSets(kdir, freq, pol, s0, B), v, z, grid=True,
+                        precision="fp32")["F"].cpu().numpy()
+    assert np.array_equal(alone, batch[0])
+    Fo = orc.force_batch(mol, kdir, freq, pol, s0, B, v, z, grid=True, want_pop=False)[0]
+    assert _map_err(batch, Fo, 16).max() < TOL32
