@@ -41,6 +41,9 @@ sys.path.insert(0, ROOT)
 
 METRIC = "16-level steady-state force evals/s and particle-steps/s: plain FP64 vs FP32+refine @1e-6"
 N_SETS, NV, NZ = 4096, 256, 256
+# dram__bytes_read.sum + dram__bytes_write.sum of one force_reduced_kernel launch
+# over the default workload (11.46 MB + 2.22 GB)
+TRAFFIC_PER_LAUNCH = 2.2315e9
 SEED = 20261203
 
 
@@ -409,7 +412,12 @@ def main():
                                         "peak": peaks["fp64"], "unit": "TFLOP/s",
                                         "frac": achieved64 / peaks["fp64"]}},
             "roofline": {"bound": "fp64+fp32", "achieved": achieved32, "peak": peak32,
-                         "unit": "TFLOP/s", "frac": achieved32 / peak32, "traffic": None,
+                         "unit": "TFLOP/s", "frac": achieved32 / peak32,
+                         # DRAM read + write of one full launch, ncu capture in
+                         # profiles/force_reduced_kernel_sroh_maps.md (4096 sets)
+                         "traffic": TRAFFIC_PER_LAUNCH if n_sets == N_SETS else None,
+                         "traffic_unit": "bytes per launch",
+                         "algorithmic_bytes": 8 * n_pts,
                          "peak_source": "mm_peak_probe FMA loop on this GPU: "
                                         f"fp64 {peaks['fp64']:.2f}, fp32 {peaks['fp32']:.2f} TFLOP/s",
                          "flops_per_point": {"fp64": f64_32, "fp32": f32_32},
