@@ -189,7 +189,13 @@ def secondary_measurements(torch, mol, pack, dev):
     ms = _ev_time(torch, lambda: traj(pack, bs1, z0, u0, 1e-6, S1), 2)
     out["traj1d"] = {"metric": "particle-steps/s", "value": 65536 * (S1 - 1) / (ms * 1e-3),
                      "particles": 65536, "steps": S1, "ms": ms,
-                     "workload": "SrOH 1D DC MOT (delta -0.2, split 0.7, s0 1, B' 0.16 T/m), Euler"}
+                     "workload": "SrOH 1D DC MOT (delta -0.2, split 0.7, s0 1, B' 0.16 T/m), Euler, "
+                                 "plain FP64 (the reference's operation order)"}
+    ms = _ev_time(torch, lambda: traj(pack, bs1, z0, u0, 1e-6, S1, precision="fp32"), 2)
+    out["traj1d_fp32"] = {"metric": "particle-steps/s", "value": 65536 * (S1 - 1) / (ms * 1e-3),
+                          "particles": 65536, "steps": S1, "ms": ms,
+                          "workload": "the same ensemble, FP32-bulk force (reduced solve), one "
+                                      "particle per thread"}
     # adjoint: 1024 parameter sets x 66 stencil points (33 z + 33 v)
     kdir, freq, pol, s0, B = make_params(mol, 1024, SEED + 7)
     bsa = BeamSets(kdir, freq, pol, s0, B)

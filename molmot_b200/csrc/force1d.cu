@@ -308,6 +308,81 @@ traj1d_kernel(ForceParams P, TrajParams T)
     }
 }
 
+// FP32-bulk trajectories: one particle per thread, the force of every step
+// from reduced_point (reduced.cuh); the same integrator, escape rule, RF
+// averaging, per-axis model and v^2 sums as traj1d_kernel.
+template <int NGMAX, int NEMAX, bool EXACT, int PAD>
+__global__ void __launch_bounds__(kRedThreads, MM_RED_MINB)
+traj1d_reduced_kernel(ForceParams P, TrajParams T)
+{
+    extern __shared__ __align__(16) unsigned char sm[];
+    RedLayout<NGMAX, NEMAX> Ly;
+    Ly.build(P.n_b);
+    RedView S0, S1;
+    build_reduced_tables<NGMAX, NEMAX, PAD>(P, 0, sm, Ly, S0);
+    S1 = S0;
+    if (T.n_avg == 2) build_reduced_tables<NGMAX, NEMAX, PAD>(P, 1, sm + Ly.total, Ly, S1);
+    const double Bg0 = P.bgrad[0], Bg1 = (T.n_avg == 2) ? P.bgrad[1] : 0.0;
+    const int nd = T.ndim;
+    const long long ip = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = ip < T.n_particles;
+    double x[3] = {0.0, 0.0, 0.0}, u[3] = {0.0, 0.0, 0.0};
+    for (int d = 0; d < nd; d++) {
+        x[d] = valid ? T.z0[ip * nd + d] : 0.0;
+        u[d] = valid ? T.v0[ip * nd + d] : 0.0;
+    }
+    long long na = T.n_steps;
+    bool done = !valid;
+    double vsq = 0.0, nsamp = 0.0;
+    const long long row = ip * T.n_steps * nd;
+    if (valid && T.z_traj)
+        for (int d = 0; d < nd; d++) { T.z_traj[row + d] = x[d]; T.v_traj[row + d] = u[d]; }
+    for (long long j = 1; j < T.n_steps; j++) {
+        if (__all_sync(0xffffffffu, done)) break;
+        if (done) continue;
+        double acc[3];
+        for (int d = 0; d < nd; d++) {
+            // axis multipliers of B' in the per-axis model: x, y see -B'/2, z sees B'
+            const double mult = (nd == 3 && d < 2) ? -0.5 : 1.0;
+            double F = reduced_point<NGMAX, NEMAX, EXACT, PAD>(P, S0, u[d], x[d], Bg0 * mult, nullptr).F;
+            if (T.n_avg == 2)
+                F = 0.5 * __dadd_rn(F, reduced_point<NGMAX, NEMAX, EXACT, PAD>(P, S1, u[d], x[d], Bg1 * mult,
+                                                                                nullptr).F);
+            acc[d] = __ddiv_rn(F, T.mass);
+        }
+        double r2 = 0.0;
+        for (int d = 0; d < nd; d++) {
+            u[d] = __dadd_rn(u[d], __dmul_rn(acc[d], T.dt));
+            x[d] = __dadd_rn(x[d], __dmul_rn(u[d], T.dt));
+            r2 = fma(x[d], x[d], r2);
+        }
+        if (T.z_traj)
+            for (int d = 0; d < nd; d++) {
+                T.z_traj[row + j * nd + d] = x[d];
+                T.v_traj[row + j * nd + d] = u[d];
+            }
+        const bool esc = (nd == 1) ? (fabs(x[0]) > T.z_escape) : (sqrt(r2) > T.z_escape);
+        if (esc) {
+            na = j;
+            done = true;
+            if (T.z_traj)
+                for (long long s2 = j + 1; s2 < T.n_steps; s2++)
+                    for (int d = 0; d < nd; d++) {
+                        T.z_traj[row + s2 * nd + d] = x[d];
+                        T.v_traj[row + s2 * nd + d] = u[d];
+                    }
+        } else if (T.i_eq >= 0 && j >= T.i_eq) {
+            for (int d = 0; d < nd; d++) vsq = __dadd_rn(vsq, __dmul_rn(u[d], u[d]));
+            nsamp += 1.0;
+        }
+    }
+    if (valid) {
+        for (int d = 0; d < nd; d++) { T.z_final[ip * nd + d] = x[d]; T.v_final[ip * nd + d] = u[d]; }
+        T.n_actual[ip] = (int32_t)na;
+        if (T.vsq_sum) { T.vsq_sum[ip] = vsq; T.n_samp[ip] = nsamp; }
+    }
+}
+
 // Size classes: (NGMAX, NEMAX, G, EXACT).
 template <int NGMAX, int NEMAX, int G, bool EXACT>
 struct Class {
@@ -376,6 +451,22 @@ int launch_reduced(const ForceParams &P, long long pts_per_set, cudaStream_t st)
     dim3 grid((unsigned)gx, (unsigned)std::min(P.n_sets, 65535));
     kern<<<grid, kRedThreads, sb, st>>>(P);
     return mm_cuda_check(cudaGetLastError(), "force_reduced_kernel launch") ? -3 : 0;
+}
+
+template <class C, int PAD>
+int launch_traj_reduced(const ForceParams &P, const TrajParams &T, cudaStream_t st)
+{
+    auto kern = traj1d_reduced_kernel<C::ng, C::ne, C::exact, PAD>;
+    RedLayout<C::ng, C::ne> Ly;
+    Ly.build(P.n_b);
+    const size_t sb = Ly.total * T.n_avg;
+    if (sb > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb);
+        if (mm_cuda_check(e, "cudaFuncSetAttribute")) return -3;
+    }
+    const long long gx = (T.n_particles + kRedThreads - 1) / kRedThreads;
+    kern<<<(unsigned)gx, kRedThreads, sb, st>>>(P, T);
+    return mm_cuda_check(cudaGetLastError(), "traj1d_reduced_kernel launch") ? -3 : 0;
 }
 
 template <class C>
@@ -593,7 +684,9 @@ extern "C" int mm_traj_run(const mm_pack *pack, const mm_beams *beams, const mm_
     cudaStream_t st = (cudaStream_t)stream;
     return dispatch_class(P.n_g, P.n_e, [&](auto C) -> int {
         using CT = decltype(C);
-        return fp32 ? launch_traj<CT, true>(P, T, st) : launch_traj<CT, false>(P, T, st);
+        if (!fp32) return launch_traj<CT, false>(P, T, st);
+        return reduced_list_granule(pack, beams) == kRedPad ? launch_traj_reduced<CT, kRedPad>(P, T, st)
+                                                            : launch_traj_reduced<CT, 1>(P, T, st);
     });
 }
 

@@ -143,3 +143,44 @@ def test_list_granules_agree(mol, pack):
     assert np.array_equal(alone, batch[0])
     Fo = orc.force_batch(mol, kdir, freq, pol, s0, B, v, z, grid=True, want_pop=False)[0]
     assert _map_err(batch, Fo, 16).max() < TOL32
+
+
+def _traj_cmp(a, b):
+    same = a["n_actual"].cpu().numpy() == b["n_actual"].cpu().numpy()
+    dz = np.abs(a["r_final"].cpu().numpy() - b["r_final"].cpu().numpy())[same]
+    dv = np.abs(a["v_final"].cpu().numpy() - b["v_final"].cpu().numpy())[same]
+    return same.mean(), dz.max(), dv.max()
+
+
+def test_fp32_trajectories_follow_fp64(mol, pack):
+    """FP32-bulk trajectories (one particle per thread, reduced solve) against
+    the plain FP64 ones: the reference's 100-particle 1D batch over 30,000
+    steps, and 3000-step runs of the per-axis 3D model and of the RF
+    two-phase average.  Escape steps agree for (nearly) every particle and the
+    end states agree closely; the MOT damps the difference of the forces."""
+    from conftest import golden
+    import bench
+    from molmot_b200.engine import BeamSets, traj
+    g = golden("trajectory_golden.npz")
+    bs = BeamSets(g["kdir"], g["freq"], g["pol"], g["s0"], float(g["B_gradient"]))
+    dt = float(g["dt"])
+    n_steps = int(float(g["t_max"]) / dt)
+    a = traj(pack, bs, g["batch_z0"], g["batch_v0"], dt, n_steps, precision="fp64")
+    b = traj(pack, bs, g["batch_z0"], g["batch_v0"], dt, n_steps, precision="fp32")
+    frac, dz, dv = _traj_cmp(a, b)
+    assert frac >= 0.98 and dz < 1e-7 and dv < 1e-4, (frac, dz, dv)
+    rng = np.random.default_rng(4)
+    r0 = rng.normal(0, 2e-3, (64, 3))
+    v0 = rng.normal(0, 0.5, (64, 3))
+    a = traj(pack, bs, r0, v0, dt, 3000, ndim=3, precision="fp64")
+    b = traj(pack, bs, r0, v0, dt, 3000, ndim=3, precision="fp32")
+    frac, dz, dv = _traj_cmp(a, b)
+    assert frac >= 0.98 and dz < 1e-7 and dv < 1e-4, (frac, dz, dv)
+    kdir, freq, pol, s0, B = bench.make_params(mol, 2, 8)
+    B[1] = -B[0]
+    rf = BeamSets(kdir, freq, pol, s0, B)
+    a = traj(pack, rf, r0[:, 2], v0[:, 2], dt, 3000, n_avg=2, i_eq=1000, precision="fp64")
+    b = traj(pack, rf, r0[:, 2], v0[:, 2], dt, 3000, n_avg=2, i_eq=1000, precision="fp32")
+    frac, dz, dv = _traj_cmp(a, b)
+    assert frac >= 0.98 and dz < 1e-7 and dv < 1e-4, (frac, dz, dv)
+    assert np.allclose(a["vsq_sum"].cpu().numpy(), b["vsq_sum"].cpu().numpy(), rtol=1e-4)
