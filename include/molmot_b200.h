@@ -41,6 +41,9 @@ extern "C" {
 #define MM_PREC_FP32_REFINE 1  /* FP32-bulk: FP32 Lorentzians with FP64 sums; force batches solve
                                   the populations in FP64 through the excited-state chain
                                   (reduced.cuh), trajectories by FP64 LU + 1 refinement step */
+#define MM_PREC_FP64_REDUCED 2 /* mm_force_batch only: FP64 rates in the plain form's operation order,
+                                  populations from the same FP64 excited-chain solve as
+                                  MM_PREC_FP32_REFINE (agrees with MM_PREC_FP64 to rounding) */
 
 /* point layouts of mm_force_batch */
 #define MM_LAYOUT_POINTS 0 /* v[i], z[i]; point i belongs to set i / points_per_set */

@@ -17,6 +17,7 @@ MM_MAX_EXCITED = 16
 MM_MAX_BEAMS = 32
 MM_PREC_FP64 = 0
 MM_PREC_FP32_REFINE = 1
+MM_PREC_FP64_REDUCED = 2
 MM_LAYOUT_POINTS = 0
 MM_LAYOUT_GRID = 1
 MM_ST_PIVOT = 1

@@ -151,7 +151,7 @@ force_adjoint_kernel(ForceParams P, double *grad)
 
 constexpr int kRedThreads = MM_RED_THREADS;
 
-template <int NGMAX, int NEMAX, bool EXACT, int PAD>
+template <int NGMAX, int NEMAX, bool EXACT, int PAD, bool F64>
 __global__ void __launch_bounds__(kRedThreads, MM_RED_MINB)
 force_reduced_kernel(ForceParams P)
 {
@@ -166,8 +166,9 @@ force_reduced_kernel(ForceParams P)
         if (set_count <= 0) continue;  // uniform over the CTA
         RedView S;
         __syncthreads();
-        build_reduced_tables<NGMAX, NEMAX, PAD>(P, set, sm, Ly, S);
+        build_reduced_tables<NGMAX, NEMAX, PAD, F64>(P, set, sm, Ly, S);
         const double Bg = P.bgrad[set];
+        double *fd = (double *)(sm + Ly.total) + threadIdx.x;  // FP64 form: n_b slots, stride blockDim.x
         const long long chunk = (set_count + gridDim.x - 1) / gridDim.x;
         const long long start = (long long)blockIdx.x * chunk;
         const long long end = min(start + chunk, set_count);
@@ -188,7 +189,7 @@ force_reduced_kernel(ForceParams P)
             }
             const long long gi = set_first + ip;
             double *pop = P.pop ? P.pop + gi * P.n_g : nullptr;
-            const RedOut o = reduced_point<NGMAX, NEMAX, EXACT, PAD>(P, S, v, z, Bg, pop);
+            const RedOut o = reduced_point<NGMAX, NEMAX, EXACT, PAD, F64>(P, S, v, z, Bg, pop, fd, blockDim.x);
             P.F[gi] = o.F;
             if (P.R) P.R[gi] = o.R;
             if (P.status) P.status[gi] = o.status;
@@ -319,9 +320,9 @@ traj1d_reduced_kernel(ForceParams P, TrajParams T)
     RedLayout<NGMAX, NEMAX> Ly;
     Ly.build(P.n_b);
     RedView S0, S1;
-    build_reduced_tables<NGMAX, NEMAX, PAD>(P, 0, sm, Ly, S0);
+    build_reduced_tables<NGMAX, NEMAX, PAD, false>(P, 0, sm, Ly, S0);
     S1 = S0;
-    if (T.n_avg == 2) build_reduced_tables<NGMAX, NEMAX, PAD>(P, 1, sm + Ly.total, Ly, S1);
+    if (T.n_avg == 2) build_reduced_tables<NGMAX, NEMAX, PAD, false>(P, 1, sm + Ly.total, Ly, S1);
     const double Bg0 = P.bgrad[0], Bg1 = (T.n_avg == 2) ? P.bgrad[1] : 0.0;
     const int nd = T.ndim;
     const long long ip = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -427,13 +428,13 @@ int launch_force(const ForceParams &P, long long pts_per_set, cudaStream_t st)
     return mm_cuda_check(cudaGetLastError(), "force_kernel launch") ? -3 : 0;
 }
 
-template <class C, int PAD>
+template <class C, int PAD, bool F64>
 int launch_reduced(const ForceParams &P, long long pts_per_set, cudaStream_t st)
 {
-    auto kern = force_reduced_kernel<C::ng, C::ne, C::exact, PAD>;
+    auto kern = force_reduced_kernel<C::ng, C::ne, C::exact, PAD, F64>;
     RedLayout<C::ng, C::ne> Ly;
     Ly.build(P.n_b);
-    const size_t sb = Ly.total;
+    const size_t sb = Ly.total + (F64 ? sizeof(double) * P.n_b * kRedThreads : 0);
     if (sb > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb);
         if (mm_cuda_check(e, "cudaFuncSetAttribute")) return -3;
@@ -615,7 +616,8 @@ static int prepare_batch(const mm_pack *pack, const mm_beams *beams, const doubl
         mm_set_error("unknown layout %d", opts->layout);
         return -1;
     }
-    if (opts->precision != MM_PREC_FP64 && opts->precision != MM_PREC_FP32_REFINE) {
+    if (opts->precision != MM_PREC_FP64 && opts->precision != MM_PREC_FP32_REFINE &&
+        opts->precision != MM_PREC_FP64_REDUCED) {
         mm_set_error("unknown precision %d", opts->precision);
         return -1;
     }
@@ -633,13 +635,15 @@ extern "C" int mm_force_batch(const mm_pack *pack, const mm_beams *beams, const 
     const int prc = prepare_batch(pack, beams, v, z, n_points, opts, F, P, pps);
     if (prc <= 0) return prc;
     P.R = R; P.pop = pop; P.status = status;
-    const bool fp32 = opts->precision == MM_PREC_FP32_REFINE;
+    const int prec = opts->precision;
     cudaStream_t st = (cudaStream_t)stream;
     return dispatch_class(P.n_g, P.n_e, [&](auto C) -> int {
         using CT = decltype(C);
-        if (!fp32) return launch_force<CT, false>(P, pps, st);
-        return reduced_list_granule(pack, beams) == kRedPad ? launch_reduced<CT, kRedPad>(P, pps, st)
-                                                            : launch_reduced<CT, 1>(P, pps, st);
+        if (prec == MM_PREC_FP64) return launch_force<CT, false>(P, pps, st);
+        const bool pad = reduced_list_granule(pack, beams) == kRedPad;
+        if (prec == MM_PREC_FP64_REDUCED)
+            return pad ? launch_reduced<CT, kRedPad, true>(P, pps, st) : launch_reduced<CT, 1, true>(P, pps, st);
+        return pad ? launch_reduced<CT, kRedPad, false>(P, pps, st) : launch_reduced<CT, 1, false>(P, pps, st);
     });
 }
 

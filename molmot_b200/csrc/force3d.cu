@@ -89,13 +89,6 @@ __device__ __forceinline__ double gsum16(double x)
     return x;
 }
 
-// Pair (p, q) of round r, slot i of the circle schedule on n (even) players.
-__device__ __forceinline__ void rr_pair(int n, int r, int i, int &p, int &q)
-{
-    auto pos = [&](int j) { return j == 0 ? 0 : ((r + j - 1) % (n - 1)) + 1; };
-    p = pos(i);
-    q = pos(n - 1 - i);
-}
 
 __device__ void load_consts3(const Force3Params &P, int set, Smem3 &S)
 {
@@ -123,6 +116,89 @@ struct Out3 {
     int status;
 };
 
+// Player at position j in round r of the circle schedule on NGM players:
+// position 0 stays, the others rotate; slot i pairs positions i and NGM-1-i.
+__host__ __device__ constexpr int rr_player(int r, int j)
+{
+    return j == 0 ? 0 : ((r + j - 1) % (NGM - 1)) + 1;
+}
+
+// One round of NGM/2 disjoint complex Jacobi rotations (H <- J^H H J,
+// V <- V J, J = [[c, s], [-conj(s), c]] on columns p, q).  Lanes 0..NGM/2-1
+// compute the rotations; then lane t updates row t of H and V (columns p, q of
+// every pair) and column t of H (rows p, q).  Every index is a compile-time
+// constant except t.
+template <int RND>
+__device__ __forceinline__ void jacobi_round(Smem3::Group &W, int t)
+{
+    constexpr int NP = NGM / 2;
+    if (t < NP) {
+        const int p = rr_player(RND, t), q = rr_player(RND, NGM - 1 - t);
+        double c = 1.0, sr = 0.0, si = 0.0;
+        const double a = W.Hre[p * LDH + p], b = W.Hre[q * LDH + q];
+        const double xr = W.Hre[p * LDH + q], xi = W.Him[p * LDH + q];
+        const double r2 = xr * xr + xi * xi;  // |H_pq|^2
+        const double ab = fabs(a) + fabs(b);
+        if (r2 > 1e-300 && r2 > 1e-36 * ab * ab) {
+            // tau = (b - a) / (2 |H_pq|), t = sign(tau) / (|tau| + sqrt(1 + tau^2)),
+            // c = 1 / sqrt(1 + t^2), s = t c e^{i arg H_pq}
+            const double irho = mm_rsqrt(r2);
+            const double tau = 0.5 * (b - a) * irho;
+            const double q1 = fma(tau, tau, 1.0);
+            const double tt = copysign(mm_rcp(fabs(tau) + q1 * mm_rsqrt(q1)), tau);
+            c = mm_rsqrt(fma(tt, tt, 1.0));
+            const double sv = tt * c * irho;
+            sr = sv * xr;
+            si = sv * xi;
+        }
+        W.rot[t][0] = c; W.rot[t][1] = sr; W.rot[t][2] = si;
+    }
+    __syncwarp();
+    if (t < NGM) {
+        // columns p, q of H and V in row t:  a_p' = a_p c - a_q conj(s);  a_q' = a_p s + a_q c
+        static_for<0, NP>([&](auto ic) {
+            constexpr int i = decltype(ic)::value;
+            constexpr int p = rr_player(RND, i), q = rr_player(RND, NGM - 1 - i);
+            const double c = W.rot[i][0], sr = W.rot[i][1], si = W.rot[i][2];
+            double *Xr = W.Hre + t * LDH, *Xi = W.Him + t * LDH;
+            for (int m = 0; m < 2; m++) {
+                const double apr = Xr[p], api = Xi[p], aqr = Xr[q], aqi = Xi[q];
+                Xr[p] = apr * c - (aqr * sr + aqi * si);
+                Xi[p] = api * c - (aqi * sr - aqr * si);
+                Xr[q] = (apr * sr - api * si) + aqr * c;
+                Xi[q] = (apr * si + api * sr) + aqi * c;
+                Xr = W.Vre + t * LDH;
+                Xi = W.Vim + t * LDH;
+            }
+        });
+    }
+    __syncwarp();
+    if (t < NGM) {
+        // rows p, q of H in column t:  a_p' = c a_p - s a_q;  a_q' = conj(s) a_p + c a_q
+        static_for<0, NP>([&](auto ic) {
+            constexpr int i = decltype(ic)::value;
+            constexpr int p = rr_player(RND, i), q = rr_player(RND, NGM - 1 - i);
+            const double c = W.rot[i][0], sr = W.rot[i][1], si = W.rot[i][2];
+            const double apr = W.Hre[p * LDH + t], api = W.Him[p * LDH + t];
+            const double aqr = W.Hre[q * LDH + t], aqi = W.Him[q * LDH + t];
+            W.Hre[p * LDH + t] = c * apr - (sr * aqr - si * aqi);
+            W.Him[p * LDH + t] = c * api - (sr * aqi + si * aqr);
+            W.Hre[q * LDH + t] = (sr * apr + si * api) + c * aqr;
+            W.Him[q * LDH + t] = (sr * api - si * apr) + c * aqi;
+        });
+    }
+    __syncwarp();
+    if (t < NP) {  // exact zero of the rotated pair, real diagonal
+        const int p = rr_player(RND, t), q = rr_player(RND, NGM - 1 - t);
+        if (W.rot[t][1] != 0.0 || W.rot[t][2] != 0.0) {
+            W.Hre[p * LDH + q] = 0.0; W.Him[p * LDH + q] = 0.0;
+            W.Hre[q * LDH + p] = 0.0; W.Him[q * LDH + p] = 0.0;
+            W.Him[p * LDH + p] = 0.0; W.Him[q * LDH + q] = 0.0;
+        }
+    }
+    __syncwarp();
+}
+
 // The 3D force at (r, v) for the group of 16 lanes (lane t, base gbase).
 // pl receives the population of ground state t (t < n_g).
 __device__ Out3 force3d_point(const Force3Params &P, Smem3 &S, Smem3::Group &W, int t, int gbase,
@@ -133,7 +209,9 @@ __device__ Out3 force3d_point(const Force3Params &P, Smem3 &S, Smem3::Group &W, 
     const double G = P.Gamma;
     int stat = 0;
 
-    // 1. field and Hermitian Zeeman matrix
+    // 1. field and Hermitian Zeeman matrix, padded to NGM x NGM with zero rows
+    //    and columns beyond n_g (a padded state couples to nothing, so no
+    //    rotation ever touches it, and it is left out of the spectrum)
     const double B0 = ((-Bg * r[0]) / 2.0) * 1e4;
     const double B1 = ((-Bg * r[1]) / 2.0) * 1e4;
     const double B2 = (Bg * r[2]) * 1e4;
@@ -141,101 +219,43 @@ __device__ Out3 force3d_point(const Force3Params &P, Smem3 &S, Smem3::Group &W, 
     // only the z component of B_hat enters the polarisation weights (cos theta)
     const double bh2 = (Bm > 1e-10) ? B2 / Bm : 1.0;
     __syncwarp();
-    for (int idx = t; idx < n_g * n_g; idx += kG3) {
-        const int i = idx / n_g, j = idx % n_g;
-        const int ij = i * n_g + j, ji = j * n_g + i;
-        const double hr = (B0 * S.Zre[0][ij] + B1 * S.Zre[1][ij]) + B2 * S.Zre[2][ij];
-        const double hi = (B0 * S.Zim[0][ij] + B1 * S.Zim[1][ij]) + B2 * S.Zim[2][ij];
-        const double gr = (B0 * S.Zre[0][ji] + B1 * S.Zre[1][ji]) + B2 * S.Zre[2][ji];
-        const double gi = (B0 * S.Zim[0][ji] + B1 * S.Zim[1][ji]) + B2 * S.Zim[2][ji];
-        W.Hre[i * LDH + j] = 0.5 * (hr + gr);   // 0.5 (H + H^H)
-        W.Him[i * LDH + j] = 0.5 * (hi - gi);
-        W.Vre[i * LDH + j] = (i == j) ? 1.0 : 0.0;
-        W.Vim[i * LDH + j] = 0.0;
+    if (t < NGM) {  // lane t writes column t
+#pragma unroll
+        for (int i = 0; i < NGM; i++) {
+            double hr = 0.0, hi = 0.0;
+            if (i < n_g && t < n_g) {
+                const int ij = i * n_g + t, ji = t * n_g + i;
+                const double ar = (B0 * S.Zre[0][ij] + B1 * S.Zre[1][ij]) + B2 * S.Zre[2][ij];
+                const double ai = (B0 * S.Zim[0][ij] + B1 * S.Zim[1][ij]) + B2 * S.Zim[2][ij];
+                const double br = (B0 * S.Zre[0][ji] + B1 * S.Zre[1][ji]) + B2 * S.Zre[2][ji];
+                const double bi = (B0 * S.Zim[0][ji] + B1 * S.Zim[1][ji]) + B2 * S.Zim[2][ji];
+                hr = 0.5 * (ar + br);  // 0.5 (H + H^H)
+                hi = 0.5 * (ai - bi);
+            }
+            W.Hre[i * LDH + t] = hr;
+            W.Him[i * LDH + t] = hi;
+            W.Vre[i * LDH + t] = (i == t) ? 1.0 : 0.0;
+            W.Vim[i * LDH + t] = 0.0;
+        }
     }
     __syncwarp();
 
-    // 2. cyclic Jacobi, circle ordering
-    const int n = (n_g + 1) & ~1;  // even number of players (one dummy when n_g is odd)
-    const int npair = n / 2;
+    // 2. cyclic Jacobi, circle ordering with a compile-time schedule
     for (int sweep = 0; sweep < 30; sweep++) {
-        // convergence: off-diagonal vs diagonal squared norms
+        // convergence: off-diagonal vs diagonal squared norms (lane t: row t)
         double off = 0.0, dia = 0.0;
-        for (int idx = t; idx < n_g * n_g; idx += kG3) {
-            const int i = idx / n_g, j = idx % n_g;
-            const double a2 = W.Hre[i * LDH + j] * W.Hre[i * LDH + j] + W.Him[i * LDH + j] * W.Him[i * LDH + j];
-            if (i == j) dia += a2; else off += a2;
+        if (t < NGM) {
+#pragma unroll
+            for (int j = 0; j < NGM; j++) {
+                const double a2 = W.Hre[t * LDH + j] * W.Hre[t * LDH + j] + W.Him[t * LDH + j] * W.Him[t * LDH + j];
+                if (j == t) dia += a2; else off += a2;
+            }
         }
         off = gsum16(off);
         dia = gsum16(dia);
         const bool more = off > 1e-30 * dia && off > 1e-300;
         if (!__any_sync(FULL, more)) break;
-        for (int rnd = 0; rnd < n - 1; rnd++) {
-            if (t < npair) {
-                int p, q;
-                rr_pair(n, rnd, t, p, q);
-                double c = 1.0, sr = 0.0, si = 0.0;
-                if (p < n_g && q < n_g) {
-                    const double a = W.Hre[p * LDH + p], b = W.Hre[q * LDH + q];
-                    const double xr = W.Hre[p * LDH + q], xi = W.Him[p * LDH + q];
-                    const double rho = sqrt(xr * xr + xi * xi);
-                    if (rho > 1e-300 && rho > 1e-18 * (fabs(a) + fabs(b))) {
-                        const double tau = (b - a) / (2.0 * rho);
-                        const double tt = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
-                        c = 1.0 / sqrt(1.0 + tt * tt);
-                        const double s = tt * c;
-                        sr = s * xr / rho;   // s e^{i phi}
-                        si = s * xi / rho;
-                    }
-                }
-                W.rot[t][0] = c; W.rot[t][1] = sr; W.rot[t][2] = si;
-            }
-            __syncwarp();
-            // columns p, q of H and V:  X' = X J,  J = [[c, s],[-conj(s), c]]
-            for (int w = t; w < 2 * npair * n_g; w += kG3) {
-                const int mat = w / (npair * n_g), rem = w % (npair * n_g);
-                const int pi = rem / n_g, row = rem % n_g;
-                int p, q;
-                rr_pair(n, rnd, pi, p, q);
-                if (p >= n_g || q >= n_g) continue;
-                double *Xr = mat ? W.Vre : W.Hre, *Xi = mat ? W.Vim : W.Him;
-                const double c = W.rot[pi][0], sr = W.rot[pi][1], si = W.rot[pi][2];
-                const double apr = Xr[row * LDH + p], api = Xi[row * LDH + p];
-                const double aqr = Xr[row * LDH + q], aqi = Xi[row * LDH + q];
-                // a_p' = a_p c - a_q conj(s);  a_q' = a_p s + a_q c
-                Xr[row * LDH + p] = apr * c - (aqr * sr + aqi * si);
-                Xi[row * LDH + p] = api * c - (aqi * sr - aqr * si);
-                Xr[row * LDH + q] = (apr * sr - api * si) + aqr * c;
-                Xi[row * LDH + q] = (apr * si + api * sr) + aqi * c;
-            }
-            __syncwarp();
-            // rows p, q of H:  H' = J^H H
-            for (int w = t; w < npair * n_g; w += kG3) {
-                const int pi = w / n_g, col = w % n_g;
-                int p, q;
-                rr_pair(n, rnd, pi, p, q);
-                if (p >= n_g || q >= n_g) continue;
-                const double c = W.rot[pi][0], sr = W.rot[pi][1], si = W.rot[pi][2];
-                const double apr = W.Hre[p * LDH + col], api = W.Him[p * LDH + col];
-                const double aqr = W.Hre[q * LDH + col], aqi = W.Him[q * LDH + col];
-                // a_p' = c a_p - s a_q;  a_q' = conj(s) a_p + c a_q
-                W.Hre[p * LDH + col] = c * apr - (sr * aqr - si * aqi);
-                W.Him[p * LDH + col] = c * api - (sr * aqi + si * aqr);
-                W.Hre[q * LDH + col] = (sr * apr + si * api) + c * aqr;
-                W.Him[q * LDH + col] = (sr * api - si * apr) + c * aqi;
-            }
-            __syncwarp();
-            if (t < npair) {  // exact zero of the rotated pair, real diagonal
-                int p, q;
-                rr_pair(n, rnd, t, p, q);
-                if (p < n_g && q < n_g && (W.rot[t][1] != 0.0 || W.rot[t][2] != 0.0)) {
-                    W.Hre[p * LDH + q] = 0.0; W.Him[p * LDH + q] = 0.0;
-                    W.Hre[q * LDH + p] = 0.0; W.Him[q * LDH + p] = 0.0;
-                    W.Him[p * LDH + p] = 0.0; W.Him[q * LDH + q] = 0.0;
-                }
-            }
-            __syncwarp();
-        }
+        static_for<0, NGM - 1>([&](auto rc) { jacobi_round<decltype(rc)::value>(W, t); });
     }
     // ascending order (ties by index), as eigh returns the spectrum
     if (t < n_g) {

@@ -56,6 +56,21 @@ __device__ __forceinline__ double mm_rcp(double d)
     return fma(y, e, y);
 }
 
+// Reciprocal square root by Newton-Raphson iteration y <- y (3 - x y^2) / 2,
+// written as e = 1/2 - (x/2) y y, y <- y + y e, started from the PTX hardware
+// approximation rsqrt.approx.ftz.f64; two steps reach double precision.
+// x must be a normal, finite, positive number.
+__device__ __forceinline__ double mm_rsqrt(double x)
+{
+    double y;
+    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    const double h = 0.5 * x;
+    double e = fma(-h * y, y, 0.5);
+    y = fma(y, e, y);
+    e = fma(-h * y, y, 0.5);
+    return fma(y, e, y);
+}
+
 // Single-precision reciprocal: hardware approximation plus one Newton step.
 __device__ __forceinline__ float mm_rcpf(float d)
 {

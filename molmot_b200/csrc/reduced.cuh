@@ -53,11 +53,34 @@ struct TripR {
     double hc1;  // hbar k kdir_b c1
 };
 
+// The same triple for the FP64 form (MM_PREC_FP64_REDUCED): the Lorentzian
+// follows the reference's detuning chain from the point's Doppler-shifted
+// beam frequency fd[b] and Zeeman-shifted energies.
+struct TripD {
+    double c1;   // ((Gamma/2) s0_b) d2 Geff
+    double c2;   // s0_b d2
+    double hk;   // (hbar k) kdir_b
+    int b, pad;
+};
+static_assert(sizeof(TripR) == 32 && sizeof(TripD) == 32, "triple records are 32 bytes");
+
+// Per-point inputs of the rate loop.  FP32 form: v and B (Gauss) in FP32.
+// FP64 form: B, the Doppler-shifted beam frequencies fd[b * stride] (this
+// thread's slots of a shared-memory scratch) and the excited energies.
+template <int NEMAX>
+struct RateCtx {
+    float vf, Bf;
+    double B;
+    const double *fd;
+    int stride;
+    double Ese[NEMAX];
+};
+
 template <int NGMAX, int NEMAX>
 struct RedLayout {
     // offs[g*NEMAX + e] .. offs[g*NEMAX + e + 1]: triples of (g, e), beams ascending
     static constexpr int n_offs = NGMAX * NEMAX + 1;
-    size_t offs, brt, rsum, flags, trip, total;
+    size_t offs, brt, rsum, flags, E, czd, zde, freq, ck, trip, total;
     __host__ __device__ static size_t al(size_t x) { return (x + 15) & ~size_t(15); }
     __host__ __device__ void build(int n_b)
     {
@@ -66,6 +89,11 @@ struct RedLayout {
         brt = o;   o = al(o + sizeof(double) * NGMAX * NEMAX);   // BR[e,g] at [g][e]
         rsum = o;  o = al(o + sizeof(double) * NEMAX);           // sum_g BR[e,g]
         flags = o; o = al(o + sizeof(int) * 4);
+        E = o;     o = al(o + sizeof(double) * (NGMAX + NEMAX));  // FP64 form: energies,
+        czd = o;   o = al(o + sizeof(double) * NGMAX);            // zd_g Gamma / 2pi,
+        zde = o;   o = al(o + sizeof(double) * NEMAX);            // zd_e,
+        freq = o;  o = al(o + sizeof(double) * n_b);              // beam frequencies,
+        ck = o;    o = al(o + sizeof(double) * n_b);              // -k kdir_b
         trip = o;  o = al(o + sizeof(TripR) * (size_t)NGMAX * NEMAX *
                                   (size_t)((n_b + kRedPad - 1) / kRedPad * kRedPad));
         total = o;
@@ -75,13 +103,14 @@ struct RedLayout {
 struct RedView {
     const int *offs;
     const double *brt, *rsum;
-    const TripR *trip;
+    const double *E, *czd, *zde, *freq, *ck;
+    const void *trip;  // TripR (FP32 form) or TripD (FP64 form)
     int valid;
 };
 
 // Parameter-set tables for the reduced kernel (all threads of the CTA);
 // lists padded to multiples of PAD.
-template <int NGMAX, int NEMAX, int PAD>
+template <int NGMAX, int NEMAX, int PAD, bool F64>
 __device__ void build_reduced_tables(const ForceParams &P, int set, unsigned char *sm,
                                      const RedLayout<NGMAX, NEMAX> &Ly, RedView &S)
 {
@@ -89,6 +118,9 @@ __device__ void build_reduced_tables(const ForceParams &P, int set, unsigned cha
     int *offs = (int *)(sm + Ly.offs), *flags = (int *)(sm + Ly.flags);
     double *brt = (double *)(sm + Ly.brt), *rsum = (double *)(sm + Ly.rsum);
     TripR *trip = (TripR *)(sm + Ly.trip);
+    TripD *tripd = (TripD *)(sm + Ly.trip);
+    double *Es = (double *)(sm + Ly.E), *czd = (double *)(sm + Ly.czd), *zde = (double *)(sm + Ly.zde);
+    double *frq = (double *)(sm + Ly.freq), *ck = (double *)(sm + Ly.ck);
     const int tid = threadIdx.x, nt = blockDim.x;
     const int32_t *pol = P.pol + (size_t)set * n_b;
     const double *kdir = P.kdir + (size_t)set * n_b, *fr = P.freq + (size_t)set * n_b;
@@ -139,6 +171,13 @@ __device__ void build_reduced_tables(const ForceParams &P, int set, unsigned cha
         flags[0] = valid;
     }
     __syncthreads();
+    for (int i = tid; i < n_g + n_e; i += nt) Es[i] = P.E[i];
+    for (int i = tid; i < n_g; i += nt) czd[i] = P.zd[i] * P.Gamma / MM_TWO_PI;
+    for (int i = tid; i < n_e; i += nt) zde[i] = P.zd[n_g + i];
+    for (int b = tid; b < n_b; b += nt) {
+        frq[b] = fr[b];
+        ck[b] = __dmul_rn(-P.k, kdir[b]);
+    }
     const double cu = MM_TWO_PI / (P.Gamma / 2.0);
     const double gh = P.Gamma / 2.0;
     for (int i = tid; i < NGMAX * NEMAX; i += nt) {
@@ -148,22 +187,38 @@ __device__ void build_reduced_tables(const ForceParams &P, int set, unsigned cha
         for (int b = 0; b < n_b; b++) {
             const double d2 = P.d2[(g * n_e + e) * 3 + pol[b]];
             if (d2 < 1e-15) continue;
-            TripR tr;
-            tr.u0 = (float)((fr[b] - (P.E[n_g + e] - P.E[g])) * cu);
-            tr.uv = (float)((-P.k * kdir[b]) / MM_TWO_PI * cu);
-            tr.uB = (float)((P.zd[n_g + e] - P.zd[g]) * P.Gamma / MM_TWO_PI * cu);
-            tr.c2 = (float)(s0[b] * d2);
-            tr.c1 = gh * s0[b] * d2 * P.geff;
-            tr.hc1 = P.hbar * P.k * kdir[b] * tr.c1;
-            trip[o++] = tr;
+            if constexpr (F64) {  // the plain form's products, in its order
+                TripD tr;
+                tr.c1 = __dmul_rn(__dmul_rn(gh, s0[b]), d2) * P.geff;
+                tr.c2 = __dmul_rn(s0[b], d2);
+                tr.hk = __dmul_rn(__dmul_rn(P.hbar, P.k), kdir[b]);
+                tr.b = b;
+                tr.pad = 0;
+                tripd[o++] = tr;
+            } else {
+                TripR tr;
+                tr.u0 = (float)((fr[b] - (P.E[n_g + e] - P.E[g])) * cu);
+                tr.uv = (float)((-P.k * kdir[b]) / MM_TWO_PI * cu);
+                tr.uB = (float)((P.zd[n_g + e] - P.zd[g]) * P.Gamma / MM_TWO_PI * cu);
+                tr.c2 = (float)(s0[b] * d2);
+                tr.c1 = gh * s0[b] * d2 * P.geff;
+                tr.hc1 = P.hbar * P.k * kdir[b] * tr.c1;
+                trip[o++] = tr;
+            }
         }
-        for (; o < offs[i + 1]; o++) {  // zero-weight padding: L = 1, every term 0
-            TripR tr = {};
-            trip[o] = tr;
+        for (; o < offs[i + 1]; o++) {  // zero-weight padding: every term 0
+            if constexpr (F64) {
+                TripD tr = {};
+                tripd[o] = tr;
+            } else {
+                TripR tr = {};
+                trip[o] = tr;
+            }
         }
     }
     __syncthreads();
     S.offs = offs; S.brt = brt; S.rsum = rsum; S.trip = trip; S.valid = flags[0];
+    S.E = Es; S.czd = czd; S.zde = zde; S.freq = frq; S.ck = ck;
 }
 
 struct RedOut {
@@ -184,28 +239,53 @@ __device__ __forceinline__ void reduced_triple(const TripR &tr, float vf, float 
     f = fma(tr.hc1, Ld, f);
 }
 
+// One triple of the FP64 form: the plain form's detuning and Lorentzian
+// (rate_equations_jit.py:58-83 operation order).
+__device__ __forceinline__ void reduced_triple64(const TripD &tr, double fdb, double Ese, double Esg,
+                                                 double gh2, double &acc, double &f, double &s)
+{
+    const double om = __dsub_rn(Ese, Esg);
+    const double de = __dmul_rn(__dsub_rn(fdb, om), MM_TWO_PI);
+    const double L = gh2 * mm_rcp(fma(de, de, gh2));
+    const double ru = tr.c1 * L;
+    acc += ru;
+    f = fma(tr.hk, ru, f);
+    s = fma(tr.c2, L, s);
+}
+
 // Rates of ground state g at one point: unsaturated FP64 sums over the
-// triples of each excited state, the force sum, and the saturation sum.
-// PAD: the list granule (kRedPad or 1).
-template <int NEMAX, int PAD>
-__device__ __forceinline__ void reduced_rates(const RedView &S, int g, float vf, float Bf,
-                                              double (&Re)[NEMAX], double &f, float &s)
+// triples of each excited state, the force sum, and the saturation sum
+// (FP32 in the FP32 form).  PAD: the list granule (kRedPad or 1).
+template <int NEMAX, int PAD, bool F64>
+__device__ __forceinline__ void reduced_rates(const RedView &S, int g, const RateCtx<NEMAX> &C,
+                                              double gh2, double (&Re)[NEMAX], double &f,
+                                              std::conditional_t<F64, double, float> &s)
 {
     f = 0.0;
-    s = 0.f;
+    s = 0;
+    double Esg = 0.0;
+    if constexpr (F64) Esg = fma(C.B, S.czd[g], S.E[g]);  // |error| <= 1 ulp of E_g
 #pragma unroll
     for (int e = 0; e < NEMAX; e++) {
         double acc = 0.0;
         const int i1 = S.offs[g * NEMAX + e + 1];
+        auto one = [&](int i) {
+            if constexpr (F64) {
+                const TripD tr = ((const TripD *)S.trip)[i];
+                reduced_triple64(tr, C.fd[tr.b * C.stride], C.Ese[e], Esg, gh2, acc, f, s);
+            } else {
+                reduced_triple(((const TripR *)S.trip)[i], C.vf, C.Bf, acc, f, s);
+            }
+        };
         if constexpr (PAD > 1) {
 #pragma unroll 1
             for (int i = S.offs[g * NEMAX + e]; i < i1; i += PAD) {
 #pragma unroll
-                for (int j = 0; j < PAD; j++) reduced_triple(S.trip[i + j], vf, Bf, acc, f, s);
+                for (int j = 0; j < PAD; j++) one(i + j);
             }
         } else {
 #pragma unroll 4
-            for (int i = S.offs[g * NEMAX + e]; i < i1; i++) reduced_triple(S.trip[i], vf, Bf, acc, f, s);
+            for (int i = S.offs[g * NEMAX + e]; i < i1; i++) one(i);
         }
         Re[e] = acc;
     }
@@ -249,16 +329,16 @@ __device__ __forceinline__ bool gth_stationary(double (&K)[NEMAX][NEMAX], int n_
 
 // Dense fallback: the reference's elimination (rate_equations_jit.py:92-136)
 // in FP64 on the same FP32-bulk rates, one point per thread (local memory).
-template <int NGMAX, int NEMAX, int PAD>
-__device__ __noinline__ RedOut dense_point(const ForceParams &P, const RedView &S, float vf, float Bf,
-                                           double *pop_out)
+template <int NGMAX, int NEMAX, int PAD, bool F64>
+__device__ __noinline__ RedOut dense_point(const ForceParams &P, const RedView &S,
+                                           const RateCtx<NEMAX> &C, double *pop_out)
 {
     const int n_g = P.n_g, n_e = P.n_e;
     double R[NGMAX][NEMAX], Fk[NGMAX], Rk[NGMAX];
     for (int g = 0; g < n_g; g++) {
         double Re[NEMAX], f;
-        float s;
-        reduced_rates<NEMAX, PAD>(S, g, vf, Bf, Re, f, s);
+        std::conditional_t<F64, double, float> s;
+        reduced_rates<NEMAX, PAD, F64>(S, g, C, (P.Gamma / 2.0) * (P.Gamma / 2.0), Re, f, s);
         const double sat = 1.0 / (1.0 + (double)s);
         double rs = 0.0;
         for (int e = 0; e < NEMAX; e++) { R[g][e] = Re[e] * sat; rs += R[g][e]; }
@@ -319,14 +399,32 @@ __device__ __noinline__ RedOut dense_point(const ForceParams &P, const RedView &
 }
 
 // One point by the reduced solve.  pop_out (nullable): n_g populations.
-template <int NGMAX, int NEMAX, bool EXACT, int PAD>
+// fd (FP64 form only): this thread's first slot of a shared scratch of n_b
+// doubles at the given stride, for the point's Doppler-shifted frequencies.
+template <int NGMAX, int NEMAX, bool EXACT, int PAD, bool F64 = false>
 __device__ __forceinline__ RedOut reduced_point(const ForceParams &P, const RedView &S, double v,
-                                                double z, double Bgrad, double *pop_out)
+                                                double z, double Bgrad, double *pop_out,
+                                                double *fd = nullptr, int stride = 0)
 {
     const int n_g = EXACT ? NGMAX : P.n_g;
     const int n_e = EXACT ? NEMAX : P.n_e;
-    const float vf = (float)v;
-    const float Bf = (float)__dmul_rn(__dmul_rn(Bgrad, z), 1e4);
+    RateCtx<NEMAX> C;
+    C.B = __dmul_rn(__dmul_rn(Bgrad, z), 1e4);
+    C.vf = (float)v;
+    C.Bf = (float)C.B;
+    C.fd = fd;
+    C.stride = stride;
+    if constexpr (F64) {
+        // laser frequency seen by the moving molecule and Zeeman-shifted
+        // excited energies, in the reference's order (exact roundings)
+        for (int b = 0; b < P.n_b; b++)
+            fd[b * stride] = __dadd_rn(S.freq[b], __ddiv_rn(__dmul_rn(S.ck[b], v), MM_TWO_PI));
+#pragma unroll
+        for (int e = 0; e < NEMAX; e++)
+            C.Ese[e] = (e < n_e) ? __dadd_rn(S.E[n_g + e], __ddiv_rn(__dmul_rn(__dmul_rn(C.B, S.zde[e]), P.Gamma),
+                                                                      MM_TWO_PI))
+                                 : 0.0;
+    }
     if (!(isfinite(v) && isfinite(z))) {  // the rate chain assumes finite, normal Lorentzians
         RedOut o;
         o.F = o.R = __longlong_as_double(0x7ff8000000000000ll);
@@ -335,7 +433,8 @@ __device__ __forceinline__ RedOut reduced_point(const ForceParams &P, const RedV
             for (int g = 0; g < n_g; g++) pop_out[g] = o.F;
         return o;
     }
-    if (!S.valid) return dense_point<NGMAX, NEMAX, PAD>(P, S, vf, Bf, pop_out);
+    if (!S.valid) return dense_point<NGMAX, NEMAX, PAD, F64>(P, S, C, pop_out);
+    const double gh2 = (P.Gamma / 2.0) * (P.Gamma / 2.0);
 
     double K[NEMAX][NEMAX], cw[NEMAX], cf[NEMAX];
 #pragma unroll
@@ -347,8 +446,8 @@ __device__ __forceinline__ RedOut reduced_point(const ForceParams &P, const RedV
     }
     for (int g = 0; g < n_g; g++) {
         double Re[NEMAX], f;
-        float s;
-        reduced_rates<NEMAX, PAD>(S, g, vf, Bf, Re, f, s);
+        std::conditional_t<F64, double, float> s;
+        reduced_rates<NEMAX, PAD, F64>(S, g, C, gh2, Re, f, s);
         double rt = 0.0;
 #pragma unroll
         for (int e = 0; e < NEMAX; e++) rt += Re[e];

@@ -19,7 +19,7 @@ from . import _lib
 from .constants import HBAR_JIT
 
 PRECISIONS = {"fp64": _lib.MM_PREC_FP64, "fp32": _lib.MM_PREC_FP32_REFINE,
-              "fp32_refine": _lib.MM_PREC_FP32_REFINE}
+              "fp32_refine": _lib.MM_PREC_FP32_REFINE, "fp64_reduced": _lib.MM_PREC_FP64_REDUCED}
 
 
 def _np(a, dtype):

@@ -184,3 +184,32 @@ def test_fp32_trajectories_follow_fp64(mol, pack):
     frac, dz, dv = _traj_cmp(a, b)
     assert frac >= 0.98 and dz < 1e-7 and dv < 1e-4, (frac, dz, dv)
     assert np.allclose(a["vsq_sum"].cpu().numpy(), b["vsq_sum"].cpu().numpy(), rtol=1e-4)
+
+
+def test_fp64_reduced_form_matches_plain(mol, pack):
+    """MM_PREC_FP64_REDUCED: FP64 rates in the plain form's operation order,
+    populations from the excited-chain solve.  It agrees with the plain FP64
+    form (the reference's elimination) to 1e-12 of max|F| per set and with the
+    oracle to the plain form's 1e-10; on unpumped sets it falls back to the same
+    elimination and agrees to rounding."""
+    import bench
+    from molmot_b200.engine import BeamSets, force_batch
+    kdir, freq, pol, s0, B = (a[WORST_SETS] for a in bench.make_params(mol, 4096, bench.SEED))
+    bs = BeamSets(kdir, freq, pol, s0, B)
+    v = np.linspace(-10, 10, 256)[::4]
+    z = np.linspace(-1e-2, 1e-2, 256)[::4]
+    red = force_batch(pack, bs, v, z, grid=True, precision="fp64_reduced")
+    plain = force_batch(pack, bs, v, z, grid=True, precision="fp64")
+    ns = len(WORST_SETS)
+    assert _map_err(red["F"].cpu().numpy(), plain["F"].cpu().numpy(), ns).max() < 1e-12
+    assert np.max(np.abs(red["pop"].cpu().numpy() - plain["pop"].cpu().numpy())) < 1e-12
+    Fo = orc.force_batch(mol, kdir, freq, pol, s0, B, v, z, grid=True, want_pop=False)[0]
+    assert _map_err(red["F"].cpu().numpy(), Fo, ns).max() < 1e-10
+    E = mol.energies
+    freq1 = np.repeat(np.array([E[15] - E[0], E[15] - E[9]]) - 10e6, 4)
+    dark = BeamSets(np.tile([1.0, -1.0], 4)[None], freq1[None], np.full((1, 8), 1), np.full((1, 8), 2.0),
+                    [0.2])
+    a = force_batch(pack, dark, v[::8], z[::8], grid=True, precision="fp64_reduced")
+    b = force_batch(pack, dark, v[::8], z[::8], grid=True, precision="fp64")
+    assert np.max(np.abs(a["pop"].cpu().numpy() - b["pop"].cpu().numpy())) < 1e-12
+    assert np.array_equal(a["status"].cpu().numpy(), b["status"].cpu().numpy())
