@@ -209,7 +209,44 @@ def secondary_measurements(torch, mol, pack, dev):
     out["adjoint"] = {"workload": "1024 parameter sets x (33 z + 33 v) stencil points, gradients "
                                   "w.r.t. 8 beam frequencies, 8 s0 and B'",
                       "forward_ms": tf, "forward_plus_adjoint_ms": ta, "cost_ratio": ta / tf}
+    out["uneven"] = uneven_measurement(torch, dev)
     return out
+
+
+def uneven_measurement(torch, dev):
+    """The uneven batch: 2048 synthetic molecules (n_ground 4..48, n_excited
+    4..16), 64..4096 points each, in one persistent launch per size class
+    (warps per CTA from the autotuner), its CUDA-graph replay, and one launch
+    per molecule on every 8th molecule, scaled to the whole batch by points."""
+    from molmot_b200.engine import BeamSets
+    from molmot_b200.uneven import MoleculeBank, UnevenBatch, make_uneven_workload
+    mols, counts, (kd, fr, po, s0), Bu, vu, zu = make_uneven_workload(n_mol=2048, seed=SEED)
+    ub = UnevenBatch(MoleculeBank(mols), counts, BeamSets(kd, fr, po, s0, Bu))
+    vd = torch.as_tensor(vu, device=dev)
+    zd = torch.as_tensor(zu, device=dev)
+    wpc = ub.autotune(vd, zd)
+    ms_p = _ev_time(torch, lambda: ub.force(vd, zd), 3)
+    g, _, _, _ = ub.graph(vd, zd)
+    ms_g = _ev_time(torch, g.replay, 3)
+    del g
+    off = np.concatenate([[0], np.cumsum(counts)])
+    sample = list(range(0, len(mols), 8))
+    singles = []
+    for i in sample:
+        u = UnevenBatch(MoleculeBank([mols[i]]), [counts[i]],
+                        BeamSets(kd[i:i + 1], fr[i:i + 1], po[i:i + 1], s0[i:i + 1], Bu[i:i + 1]),
+                        warps_per_cta=wpc)
+        singles.append((u, vd[off[i]:off[i + 1]], zd[off[i]:off[i + 1]]))
+    ms_s = _ev_time(torch, lambda: [u.force(a, b) for u, a, b in singles], 2)
+    pts_s = int(sum(counts[i] for i in sample))
+    n = int(off[-1])
+    return {"metric": "force evals/s", "points": n, "molecules": len(mols),
+            "persistent_ms": ms_p, "persistent_value": n / (ms_p * 1e-3),
+            "graph_replay_ms": ms_g, "warps_per_cta": list(wpc),
+            "per_molecule_launches_ms_estimate": ms_s * n / pts_s,
+            "per_molecule_sample": f"{len(sample)} molecules ({pts_s} points), scaled by points",
+            "workload": "2048 synthetic molecules, n_ground 4..48, n_excited 4..16, 64..4096 "
+                        "(v, z) points each, plain FP64 (the reference's elimination)"}
 
 
 def oracle_check(mol, pack, bs, v_d, z_d, kdir, freq, pol, s0, B, sets=(0, 1, 2047, 4095)):

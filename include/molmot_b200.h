@@ -287,6 +287,28 @@ MM_API int mm_traj3d_run(const mm_pack *pack, const mm_beams *beams, const doubl
  * Used as the roofline peak of the force kernels, which are bound by the
  * FP64/FP32 CUDA-core pipes.
  */
+/*
+ * Per-time-bin statistics of a trajectory ensemble (the reductions of
+ * sigma_vs_time, temperature_vs_time and density_vs_time,
+ * molmot/mot/analysis.py:128-287).  z, v: device arrays, value of particle p
+ * at time index j at [p * stride + j]; time_index: device array of n_bins
+ * indices.  Particles with |z| < r_alive count.  out (device, [n_bins][6]):
+ * count, mean z, mean v, variance of z, variance of v (population, two-pass),
+ * mean v^2.
+ */
+MM_API int mm_ensemble_stats(const double *z, const double *v, int64_t n_particles, int64_t stride,
+                             const int64_t *time_index, int32_t n_bins, double r_alive, double *out,
+                             void *stream);
+
+/*
+ * numpy.histogram of x[i * stride], i < n, with `bins` equal bins on [lo, hi]
+ * (the histograms of gaussian_fit and maxwell_boltzmann_fit_1d,
+ * molmot/mot/analysis.py:28-125).  counts: device array of bins uint64,
+ * overwritten.
+ */
+MM_API int mm_histogram(const double *x, int64_t n, int64_t stride, double lo, double hi, int32_t bins,
+                        uint64_t *counts, void *stream);
+
 MM_API int mm_peak_probe(int32_t which, int64_t iters, double *ms_out, double *flops_out,
                          void *stream);
 

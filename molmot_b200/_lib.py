@@ -95,6 +95,10 @@ SIGNATURES = {
     "mm_uneven_force_static": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(ctypes.c_int64),
                                               ctypes.POINTER(UnevenOpts), _vp, _vp, ctypes.c_double,
                                               ctypes.c_int32, _vp, _vp, _vp, _vp]),
+    "mm_ensemble_stats": (ctypes.c_int, [_vp, _vp, ctypes.c_int64, ctypes.c_int64, _vp, ctypes.c_int32,
+                                         ctypes.c_double, _vp, _vp]),
+    "mm_histogram": (ctypes.c_int, [_vp, ctypes.c_int64, ctypes.c_int64, ctypes.c_double, ctypes.c_double,
+                                    ctypes.c_int32, _vp, _vp]),
     "mm_peak_probe": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int64, _dp, _dp, _vp]),
 }
 

@@ -206,5 +206,36 @@ def main():
     print("golden fixtures written to", HERE)
 
 
+def analysis_golden():
+    """molmot/mot/analysis.py on seeded synthetic ensembles (oracle/analysis.py
+    synthetic_ensemble), in the reference's list-of-tuples form."""
+    from molmot.mot import analysis as an
+    sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+    from oracle.analysis import synthetic_ensemble
+    out = {"versions": versions()}
+    mass = 104.0 * 1.66053906660e-27
+    for k, (seed, n, S) in enumerate([(7, 150, 600), (11, 60, 300)]):
+        t, Z, V = synthetic_ensemble(seed, n, S)
+        res = [(t, Z[i], V[i]) for i in range(n)]
+        c, sz, sv, na = an.sigma_vs_time(res, time_bins=40)
+        _, T = an.temperature_vs_time(res, mass, time_bins=40)
+        _, n0 = an.density_vs_time(res, N_total=2000, time_bins=40)
+        out.update({f"e{k}_seed": seed, f"e{k}_n": n, f"e{k}_steps": S, f"e{k}_t": c, f"e{k}_sz": sz,
+                    f"e{k}_sv": sv, f"e{k}_na": na, f"e{k}_T": T, f"e{k}_n0": n0,
+                    f"e{k}_capture": an.capture_fraction(res, r_max=3e-3, t_min=1e-3),
+                    f"e{k}_capture_t0": an.capture_fraction(res, r_max=5e-3, t_min=0.0),
+                    f"e{k}_survived": np.array([an.survived(r) for r in res]),
+                    f"e{k}_gfit": an.gaussian_fit(Z[:, S // 2]),
+                    f"e{k}_gfit_final": an.gaussian_fit(Z[:, -1], bins=80, range_mm=(-5, 5)),
+                    f"e{k}_mbfit": an.maxwell_boltzmann_fit_1d(V[:, -1], mass)})
+    out["mass"] = mass
+    np.savez(os.path.join(HERE, "analysis_golden.npz"), **out)
+    print("analysis golden written")
+
+
 if __name__ == "__main__":
-    main()
+    if len(sys.argv) > 1 and sys.argv[1] == "analysis":
+        analysis_golden()
+    else:
+        main()
+        analysis_golden()
