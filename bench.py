@@ -246,7 +246,9 @@ def uneven_measurement(torch, dev):
             "per_molecule_launches_ms_estimate": ms_s * n / pts_s,
             "per_molecule_sample": f"{len(sample)} molecules ({pts_s} points), scaled by points",
             "workload": "2048 synthetic molecules, n_ground 4..48, n_excited 4..16, 64..4096 "
-                        "(v, z) points each, plain FP64 (the reference's elimination)"}
+                        "(v, z) points each; FP64 rates in the reference's order, populations "
+                        "from the FP64 excited-chain solve (the reference's elimination for "
+                        "molecules the reduction does not cover)"}
 
 
 def oracle_check(mol, pack, bs, v_d, z_d, kdir, freq, pol, s0, B, sets=(0, 1, 2047, 4095)):

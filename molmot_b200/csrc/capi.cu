@@ -19,6 +19,9 @@ int mm_cuda_check(cudaError_t e, const char *what)
 {
     if (e == cudaSuccess) return 0;
     mm_set_error("%s: %s", what, cudaGetErrorString(e));
+    // the error is reported here; clear the runtime's pending copy of it so a
+    // later, unrelated check in this thread does not return it again
+    (void)cudaGetLastError();
     return 1;
 }
 

@@ -28,8 +28,7 @@
 // of max|F| on some parameter sets).  Everything after the rates is FP64.
 //
 // Degenerate sets: a ground state with no active triple (r_g = 0), or an
-// excited-state chain that the state reduction cannot eliminate in index
-// order.  Both are properties of the parameter set (which triples exist), so
+// excited-state chain that is not strongly connected.  Both are properties of the parameter set (which triples exist), so
 // the CTA decides once per set and then solves every point with
 // dense_point(), the reference's own elimination in FP64 on the same rates.
 #pragma once
@@ -143,26 +142,28 @@ __device__ void build_reduced_tables(const ForceParams &P, int set, unsigned cha
     if (tid == 0) {
         offs[0] = 0;
         for (int i = 1; i <= NGMAX * NEMAX; i++) offs[i] = offs[i - 1] + (offs[i] + PAD - 1) / PAD * PAD;
-        // structural checks: every ground state pumped; excited chain reducible in index order
+        // structural checks: every ground state pumped, and the excited-state
+        // chain (e' -> e when e' decays to a ground state that a beam excites
+        // to e) strongly connected, so its stationary vector is unique and
+        // the state reduction never meets a zero outflow
         int valid = 1;
         for (int g = 0; g < n_g; g++)
             if (offs[g * NEMAX + NEMAX] == offs[g * NEMAX]) valid = 0;
-        bool T[NEMAX][NEMAX];  // T[i][j]: transition i -> j possible (decay to g, re-excitation to j)
-        for (int i = 0; i < NEMAX; i++)
-            for (int j = 0; j < NEMAX; j++) {
-                bool t = false;
-                if (i < n_e && j < n_e)
-                    for (int g = 0; g < n_g; g++)
-                        if (brt[g * NEMAX + i] > 0.0 && offs[g * NEMAX + j + 1] > offs[g * NEMAX + j]) t = true;
-                T[i][j] = t;
-            }
-        for (int k = n_e - 1; k >= 1; k--) {
-            bool s = false;
-            for (int j = 0; j < k; j++) s = s || T[k][j];
-            if (!s) valid = 0;
-            for (int i = 0; i < k; i++)
-                for (int j = 0; j < k; j++) T[i][j] = T[i][j] || (T[i][k] && T[k][j]);
+        unsigned T[NEMAX];
+        for (int i = 0; i < n_e; i++) {
+            unsigned ti = 1u << i;
+            for (int g = 0; g < n_g; g++)
+                if (brt[g * NEMAX + i] > 0.0)
+                    for (int j = 0; j < n_e; j++)
+                        if (offs[g * NEMAX + j + 1] > offs[g * NEMAX + j]) ti |= 1u << j;
+            T[i] = ti;
         }
+        for (int k = 0; k < n_e; k++)
+            for (int i = 0; i < n_e; i++)
+                if (T[i] >> k & 1u) T[i] |= T[k];
+        const unsigned all = (1u << n_e) - 1u;
+        for (int i = 0; i < n_e; i++)
+            if ((T[i] & all) != all) valid = 0;
         for (int e = 0; e < NEMAX; e++) {
             double a = 0.0;
             for (int g = 0; g < n_g; g++) a += brt[g * NEMAX + e];

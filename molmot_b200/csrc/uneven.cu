@@ -45,6 +45,7 @@ struct mm_uneven_plan {
     int n_tasks[3];
     UnevenTask *d_tasks[3];
     int *d_counter;                    // [3], reset by every mm_uneven_force
+    int *d_valid;                      // [n_mol]: the reduced solve applies (set per call)
     std::vector<UnevenTask> h_tasks[3];
 };
 
@@ -68,16 +69,24 @@ struct UnevenParams {
     int n_tasks;
     int *counter;
     int persistent;
+    // valid[m] = 1: molecule m is solved by the reduced kernels; the
+    // elimination kernels then take only molecules with valid[m] = 0.
+    // nullptr: the elimination kernels take every molecule.
+    const int *valid;
 };
 
-template <int NGMAX, int NEMAX>
+template <int NGMAX, int NEMAX, bool RED = false>
 struct ULayout {
     static constexpr int LDA = NGMAX + 1;
+    static constexpr int LDK = NEMAX + 1;
     // per CTA
     static constexpr int mol_doubles = 2 * (NGMAX + NEMAX) + NGMAX * NEMAX * 3 + NEMAX * NGMAX + NGMAX;
     static constexpr int beam_doubles = 5 * NBU;
     // per group
-    static constexpr int grp_doubles = NGMAX * LDA + NGMAX * NEMAX + 6 * NGMAX + NBU + NEMAX;
+    // elimination: A, Rm, bv, xv, invU, Fk, Rk, Esg, fd, Ese
+    // reduced:     Rm (scaled rates), K, Fk, Rk, Esg, w, phi, fd, Ese, cw, cf, rs, pi
+    static constexpr int grp_doubles = RED ? NGMAX * NEMAX + NEMAX * LDK + 5 * NGMAX + NBU + 5 * NEMAX
+                                           : NGMAX * LDA + NGMAX * NEMAX + 6 * NGMAX + NBU + NEMAX;
     static size_t bytes(int groups)
     {
         return sizeof(double) * (size_t)(mol_doubles + beam_doubles + groups * grp_doubles) +
@@ -91,12 +100,17 @@ __device__ __forceinline__ double gsum(double x, int G)
     return x;
 }
 
-template <int NGMAX, int NEMAX, int G>
+// RED: the populations from the excited-state chain (see reduced.cuh for the
+// identity): each group scales its rates by 1/r_g, forms K = A^T BR^T
+// (n_e x n_e) and the two n_e-vectors in shared memory, reduces the chain
+// cooperatively and writes F and R.  Molecules the reduction does not cover
+// (valid[m] = 0) are left to the elimination kernels (RED = false).
+template <int NGMAX, int NEMAX, int G, bool RED>
 __global__ void __launch_bounds__(256)
 uneven_kernel(UnevenParams P)
 {
-    using Ly = ULayout<NGMAX, NEMAX>;
-    constexpr int LDA = Ly::LDA;
+    using Ly = ULayout<NGMAX, NEMAX, RED>;
+    constexpr int LDA = Ly::LDA, LDK = Ly::LDK;
     extern __shared__ __align__(16) unsigned char smraw[];
     double *smd = (double *)smraw;
     // molecule
@@ -112,9 +126,19 @@ uneven_kernel(UnevenParams P)
     const int lane = threadIdx.x & 31, t = lane % G;
     const int group = threadIdx.x / G;
     double *W = grp0 + (size_t)group * Ly::grp_doubles;
-    double *A = W, *Rm = A + NGMAX * LDA, *bv = Rm + NGMAX * NEMAX, *xv = bv + NGMAX;
-    double *invU = xv + NGMAX, *Fk = invU + NGMAX, *Rk = Fk + NGMAX, *Esg = Rk + NGMAX;
-    double *fd = Esg + NGMAX, *Ese = fd + NBU;
+    double *A, *Rm, *bv, *xv, *invU, *Fk, *Rk, *Esg, *fd, *Ese;
+    double *Kc = nullptr, *wg = nullptr, *ph = nullptr, *cw = nullptr, *cf = nullptr, *rsv = nullptr,
+           *piv = nullptr;
+    if constexpr (RED) {
+        Rm = W; Kc = Rm + NGMAX * NEMAX; Fk = Kc + NEMAX * LDK; Rk = Fk + NGMAX; Esg = Rk + NGMAX;
+        wg = Esg + NGMAX; ph = wg + NGMAX; fd = ph + NGMAX; Ese = fd + NBU;
+        cw = Ese + NEMAX; cf = cw + NEMAX; rsv = cf + NEMAX; piv = rsv + NEMAX;
+        A = bv = xv = invU = nullptr;
+    } else {
+        A = W; Rm = A + NGMAX * LDA; bv = Rm + NGMAX * NEMAX; xv = bv + NGMAX;
+        invU = xv + NGMAX; Fk = invU + NGMAX; Rk = Fk + NGMAX; Esg = Rk + NGMAX;
+        fd = Esg + NGMAX; Ese = fd + NBU;
+    }
     const int n_b = P.n_b;
 
     for (int it = 0;; it++) {
@@ -126,6 +150,7 @@ uneven_kernel(UnevenParams P)
         if (task >= P.n_tasks) break;
         const UnevenTask T = P.tasks[task];
         const int m = T.mol;
+        if (P.valid && (RED ? !P.valid[m] : P.valid[m])) continue;  // uniform over the CTA
         const int n_g = P.ng[m], n_e = P.ne[m], n_s = n_g + n_e;
         const double Gam = P.gam[m], kw = P.kw[m];
         const double *mb = P.buf + P.off[m];
@@ -188,102 +213,209 @@ uneven_kernel(UnevenParams P)
                 Rk[k] = rs;
             }
             __syncwarp();
-            // population matrix M' (rows i, columns j), right-hand side e_last
-            for (int i = 0; i < n_g; i++) {
-                for (int j = t; j < n_g; j += G) {
-                    double a = (i == j) ? -Rk[j] : 0.0;
-                    for (int e = 0; e < n_e; e++) a = fma(Rm[j * NEMAX + e], BR[e * n_g + i], a);
-                    A[i * LDA + j] = (i == n_g - 1) ? 1.0 : a;
+            if constexpr (RED) {
+                // a_ge = R[g,e] / r_g, w_g = 1 / r_g, phi_g = F_g / r_g (lane per ground state)
+                for (int k = t; k < n_g; k += G) {
+                    const double inv = mm_rcp(Rk[k]);  // r_g > 0: every ground state is pumped
+                    for (int e = 0; e < n_e; e++) Rm[k * NEMAX + e] *= inv;
+                    wg[k] = inv;
+                    ph[k] = Fk[k] * inv;
                 }
-            }
-            for (int i = t; i < n_g; i += G) bv[i] = (i == n_g - 1) ? 1.0 : 0.0;
-            __syncwarp();
-            // elimination with partial pivoting
-            for (int col = 0; col < n_g; col++) {
-                double best = -1.0;
-                int brow = n_g;
-                for (int r = col + t; r < n_g; r += G) {
-                    const double a = fabs(A[r * LDA + col]);
-                    if (a > best) { best = a; brow = r; }
+                __syncwarp();
+                // K[e][e'] = sum_g a_ge BR[e', g]; cw, cf, rs: sums of BR[e', g] w_g, phi_g, 1
+                for (int idx = t; idx < n_e * n_e; idx += G) {
+                    const int e = idx / n_e, e2 = idx - e * n_e;
+                    double a = 0.0;
+                    for (int g = 0; g < n_g; g++) a = fma(Rm[g * NEMAX + e], BR[e2 * n_g + g], a);
+                    Kc[e * LDK + e2] = a;
                 }
-                for (int o = G >> 1; o > 0; o >>= 1) {
-                    const double ob = __shfl_xor_sync(0xffffffffu, best, o);
-                    const int orow = __shfl_xor_sync(0xffffffffu, brow, o);
-                    if (ob > best || (ob == best && orow < brow)) { best = ob; brow = orow; }
-                }
-                const int prow = brow;
-                if (prow != col) {
-                    for (int j = t; j < n_g; j += G) {
-                        const double tmp = A[col * LDA + j];
-                        A[col * LDA + j] = A[prow * LDA + j];
-                        A[prow * LDA + j] = tmp;
+                for (int e2 = t; e2 < n_e; e2 += G) {
+                    double a = 0.0, b = 0.0, c = 0.0;
+                    for (int g = 0; g < n_g; g++) {
+                        const double br = BR[e2 * n_g + g];
+                        a = fma(br, wg[g], a);
+                        b = fma(br, ph[g], b);
+                        c += br;
                     }
-                    if (t == 0) { const double tb = bv[col]; bv[col] = bv[prow]; bv[prow] = tb; }
+                    cw[e2] = a;
+                    cf[e2] = b;
+                    rsv[e2] = c;
                 }
                 __syncwarp();
-                const double pv = A[col * LDA + col];
-                const double ap = fabs(pv);
-                const double y = mm_rcp(ap >= 1e-30 ? pv : 1.0);
-                const double inv_e = (ap < 1e-30) ? 0.0 : y;
-                if (ap < 1e-30) stat |= MM_ST_PIVOT;
-                if (t == 0) invU[col] = (ap > 1e-30) ? y : 0.0;
-                for (int r = col + 1 + t; r < n_g; r += G) A[r * LDA + col] *= inv_e;
-                __syncwarp();
-                for (int r = col + 1; r < n_g; r++) {
-                    const double f = A[r * LDA + col];
-                    for (int j = col + 1 + t; j < n_g; j += G)
-                        A[r * LDA + j] = fma(-f, A[col * LDA + j], A[r * LDA + j]);
+                // state reduction of the chain, Q[i][j] = K[j][i] (probability i -> j)
+                bool ok = true;
+                for (int k = n_e - 1; k >= 1; k--) {
+                    double S = 0.0;
+                    for (int j = 0; j < k; j++) S += Kc[j * LDK + k];
+                    ok = ok && (S > 0.0);
+                    const double inv = mm_rcp(S > 0.0 ? S : 1.0);
+                    __syncwarp();
+                    for (int i = t; i < k; i += G) Kc[k * LDK + i] *= inv;
+                    __syncwarp();
+                    for (int idx = t; idx < k * k; idx += G) {
+                        const int i = idx / k, j = idx - i * k;
+                        Kc[j * LDK + i] = fma(Kc[k * LDK + i], Kc[j * LDK + k], Kc[j * LDK + i]);
+                    }
+                    __syncwarp();
                 }
-                for (int r = col + 1 + t; r < n_g; r += G)
-                    bv[r] = fma(-A[r * LDA + col], bv[col], bv[r]);
+                double nrm = 0.0, fn = 0.0, rn = 0.0;
+                if (t == 0) {
+                    piv[0] = 1.0;
+                    for (int k = 1; k < n_e; k++) {
+                        double a = 0.0;
+                        for (int i = 0; i < k; i++) a = fma(piv[i], Kc[k * LDK + i], a);
+                        piv[k] = a;
+                    }
+                    for (int e = 0; e < n_e; e++) {
+                        nrm = fma(cw[e], piv[e], nrm);
+                        fn = fma(cf[e], piv[e], fn);
+                        rn = fma(rsv[e], piv[e], rn);
+                    }
+                    const double in = mm_rcp(nrm);
+                    const double Fo = fn * in, Ro = rn * in;
+                    int st = 0;
+                    if (!ok || !isfinite(Fo)) st |= MM_ST_NONFINITE;
+                    if (valid) {
+                        P.F[gi] = Fo;
+                        if (P.R) P.R[gi] = Ro;
+                        if (P.status) P.status[gi] = st;
+                    }
+                }
                 __syncwarp();
-            }
-            // back substitution
-            for (int i = n_g - 1; i >= 0; i--) {
-                double part = 0.0;
-                for (int j = i + 1 + t; j < n_g; j += G) part = fma(A[i * LDA + j], xv[j], part);
-                part = gsum(part, G);
-                const double xi = (bv[i] - part) * invU[i];
-                __syncwarp();
-                if (t == 0) xv[i] = xi;
-                __syncwarp();
-            }
-            // clamp, normalise, force
-            double tot = 0.0, Fs = 0.0, Rs = 0.0;
-            for (int i = t; i < n_g; i += G) {
-                const double p = xv[i] > 0.0 ? xv[i] : 0.0;
-                tot += p;
-                Fs = fma(p, Fk[i], Fs);
-                Rs = fma(p, Rk[i], Rs);
-            }
-            // uniform-population sums, reduced outside the branch (both 16-lane groups
-            // of a warp take every shuffle)
-            double fu = 0.0, ru = 0.0;
-            for (int i = t; i < n_g; i += G) { fu += Fk[i]; ru += Rk[i]; }
-            tot = gsum(tot, G);
-            Fs = gsum(Fs, G);
-            Rs = gsum(Rs, G);
-            fu = gsum(fu, G);
-            ru = gsum(ru, G);
-            double Fo, Ro;
-            if (tot > 0.0) {
-                const double it = mm_rcp(tot);
-                Fo = Fs * it;
-                Ro = Rs * it;
             } else {
-                stat |= MM_ST_ZERO_POP;
-                Fo = P.uniform_fb ? fu / n_g : 0.0;
-                Ro = P.uniform_fb ? ru / n_g : 0.0;
-            }
-            if (!isfinite(Fo)) stat |= MM_ST_NONFINITE;
-            for (int o = G >> 1; o > 0; o >>= 1) stat |= __shfl_xor_sync(0xffffffffu, stat, o);
-            if (valid && t == 0) {
-                P.F[gi] = Fo;
-                if (P.R) P.R[gi] = Ro;
-                if (P.status) P.status[gi] = stat;
+                // population matrix M' (rows i, columns j), right-hand side e_last
+                for (int i = 0; i < n_g; i++) {
+                    for (int j = t; j < n_g; j += G) {
+                        double a = (i == j) ? -Rk[j] : 0.0;
+                        for (int e = 0; e < n_e; e++) a = fma(Rm[j * NEMAX + e], BR[e * n_g + i], a);
+                        A[i * LDA + j] = (i == n_g - 1) ? 1.0 : a;
+                    }
+                }
+                for (int i = t; i < n_g; i += G) bv[i] = (i == n_g - 1) ? 1.0 : 0.0;
+                __syncwarp();
+                // elimination with partial pivoting
+                for (int col = 0; col < n_g; col++) {
+                    double best = -1.0;
+                    int brow = n_g;
+                    for (int r = col + t; r < n_g; r += G) {
+                        const double a = fabs(A[r * LDA + col]);
+                        if (a > best) { best = a; brow = r; }
+                    }
+                    for (int o = G >> 1; o > 0; o >>= 1) {
+                        const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+                        const int orow = __shfl_xor_sync(0xffffffffu, brow, o);
+                        if (ob > best || (ob == best && orow < brow)) { best = ob; brow = orow; }
+                    }
+                    const int prow = brow;
+                    if (prow != col) {
+                        for (int j = t; j < n_g; j += G) {
+                            const double tmp = A[col * LDA + j];
+                            A[col * LDA + j] = A[prow * LDA + j];
+                            A[prow * LDA + j] = tmp;
+                        }
+                        if (t == 0) { const double tb = bv[col]; bv[col] = bv[prow]; bv[prow] = tb; }
+                    }
+                    __syncwarp();
+                    const double pv = A[col * LDA + col];
+                    const double ap = fabs(pv);
+                    const double y = mm_rcp(ap >= 1e-30 ? pv : 1.0);
+                    const double inv_e = (ap < 1e-30) ? 0.0 : y;
+                    if (ap < 1e-30) stat |= MM_ST_PIVOT;
+                    if (t == 0) invU[col] = (ap > 1e-30) ? y : 0.0;
+                    for (int r = col + 1 + t; r < n_g; r += G) A[r * LDA + col] *= inv_e;
+                    __syncwarp();
+                    for (int r = col + 1; r < n_g; r++) {
+                        const double f = A[r * LDA + col];
+                        for (int j = col + 1 + t; j < n_g; j += G)
+                            A[r * LDA + j] = fma(-f, A[col * LDA + j], A[r * LDA + j]);
+                    }
+                    for (int r = col + 1 + t; r < n_g; r += G)
+                        bv[r] = fma(-A[r * LDA + col], bv[col], bv[r]);
+                    __syncwarp();
+                }
+                // back substitution
+                for (int i = n_g - 1; i >= 0; i--) {
+                    double part = 0.0;
+                    for (int j = i + 1 + t; j < n_g; j += G) part = fma(A[i * LDA + j], xv[j], part);
+                    part = gsum(part, G);
+                    const double xi = (bv[i] - part) * invU[i];
+                    __syncwarp();
+                    if (t == 0) xv[i] = xi;
+                    __syncwarp();
+                }
+                // clamp, normalise, force
+                double tot = 0.0, Fs = 0.0, Rs = 0.0;
+                for (int i = t; i < n_g; i += G) {
+                    const double p = xv[i] > 0.0 ? xv[i] : 0.0;
+                    tot += p;
+                    Fs = fma(p, Fk[i], Fs);
+                    Rs = fma(p, Rk[i], Rs);
+                }
+                // uniform-population sums, reduced outside the branch (both 16-lane groups
+                // of a warp take every shuffle)
+                double fu = 0.0, ru = 0.0;
+                for (int i = t; i < n_g; i += G) { fu += Fk[i]; ru += Rk[i]; }
+                tot = gsum(tot, G);
+                Fs = gsum(Fs, G);
+                Rs = gsum(Rs, G);
+                fu = gsum(fu, G);
+                ru = gsum(ru, G);
+                double Fo, Ro;
+                if (tot > 0.0) {
+                    const double it = mm_rcp(tot);
+                    Fo = Fs * it;
+                    Ro = Rs * it;
+                } else {
+                    stat |= MM_ST_ZERO_POP;
+                    Fo = P.uniform_fb ? fu / n_g : 0.0;
+                    Ro = P.uniform_fb ? ru / n_g : 0.0;
+                }
+                if (!isfinite(Fo)) stat |= MM_ST_NONFINITE;
+                for (int o = G >> 1; o > 0; o >>= 1) stat |= __shfl_xor_sync(0xffffffffu, stat, o);
+                if (valid && t == 0) {
+                    P.F[gi] = Fo;
+                    if (P.R) P.R[gi] = Ro;
+                    if (P.status) P.status[gi] = stat;
+                }
             }
         }
     }
+}
+
+// valid[m] = 1 when the excited-state chain reduction applies to molecule m
+// with its beam set: every ground state has an active (beam, excited) pair,
+// and the chain of excited states (e' -> e when e' decays to a ground state
+// that some beam excites to e) is strongly connected, so its stationary
+// vector is unique and the state reduction never meets a zero outflow.
+__global__ void uneven_valid_kernel(UnevenParams P, int n_mol, int *valid)
+{
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= n_mol) return;
+    const int n_g = P.ng[m], n_e = P.ne[m], n_s = n_g + n_e, n_b = P.n_b;
+    const double *mb = P.buf + P.off[m];
+    const double *d2 = mb + 2 * n_s, *BR = d2 + n_g * n_e * 3;
+    const int32_t *pol = P.pol + (size_t)m * n_b;
+    int ok = 1;
+    unsigned T[MM_MAX_EXCITED];
+    for (int e = 0; e < n_e; e++) T[e] = 0u;
+    for (int g = 0; g < n_g; g++) {
+        unsigned act = 0u;  // excited states that some beam drives from g
+        for (int e = 0; e < n_e; e++)
+            for (int b = 0; b < n_b; b++)
+                if (d2[(g * n_e + e) * 3 + pol[b]] >= 1e-15) act |= 1u << e;
+        if (!act) ok = 0;
+        for (int e = 0; e < n_e; e++)
+            if (BR[e * n_g + g] > 0.0) T[e] |= act;
+    }
+    // reachability closure (Floyd-Warshall on bit masks)
+    for (int e = 0; e < n_e; e++) T[e] |= 1u << e;
+    for (int k = 0; k < n_e; k++)
+        for (int i = 0; i < n_e; i++)
+            if (T[i] >> k & 1u) T[i] |= T[k];
+    const unsigned all = (n_e >= 32) ? 0xffffffffu : ((1u << n_e) - 1u);
+    for (int e = 0; e < n_e; e++)
+        if ((T[e] & all) != all) ok = 0;
+    valid[m] = ok;
 }
 
 template <int NGMAX, int NEMAX, int G>
@@ -302,7 +434,7 @@ int class_of(int n_g, int n_e)
     return 2;
 }
 
-template <class C>
+template <class C, bool RED = false>
 int launch_class(const UnevenParams &P0, const mm_uneven_plan *plan, int cls, int persistent,
                  cudaStream_t st)
 {
@@ -314,8 +446,16 @@ int launch_class(const UnevenParams &P0, const mm_uneven_plan *plan, int cls, in
     P.persistent = persistent;
     const int threads = 32 * plan->wpc[cls];
     const int groups = threads / C::g;
-    auto kern = uneven_kernel<C::ng, C::ne, C::g>;
-    const size_t sb = ULayout<C::ng, C::ne>::bytes(groups);
+    auto kern = uneven_kernel<C::ng, C::ne, C::g, RED>;
+    const size_t sb = ULayout<C::ng, C::ne, RED>::bytes(groups);
+    int dev0 = 0, smax = 0;
+    cudaGetDevice(&dev0);
+    cudaDeviceGetAttribute(&smax, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev0);
+    if (sb > (size_t)smax) {
+        mm_set_error("size class %d at %d warps per CTA needs %zu bytes of shared memory (limit %d)", cls,
+                     plan->wpc[cls], sb, smax);
+        return -1;
+    }
     if (mm_cuda_check(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb),
                       "cudaFuncSetAttribute"))
         return -3;
@@ -448,6 +588,7 @@ extern "C" int mm_uneven_plan_create(const mm_bank *bank, const int64_t *point_o
         }
     }
     rc |= mm_cuda_check(cudaMalloc((void **)&p->d_counter, 3 * sizeof(int)), "cudaMalloc");
+    rc |= mm_cuda_check(cudaMalloc((void **)&p->d_valid, sizeof(int) * n_mol), "cudaMalloc");
     if (rc) { mm_uneven_plan_destroy(p); return -3; }
     *out = p;
     return 0;
@@ -458,6 +599,7 @@ extern "C" int mm_uneven_plan_destroy(mm_uneven_plan *p)
     if (!p) return 0;
     for (int c = 0; c < 3; c++) cudaFree(p->d_tasks[c]);
     cudaFree(p->d_counter);
+    cudaFree(p->d_valid);
     delete p;
     return 0;
 }
@@ -483,10 +625,20 @@ extern "C" int mm_uneven_force(const mm_uneven_plan *plan, const mm_beams *beams
     P.hbar = hbar > 0 ? hbar : MM_HBAR_JIT;
     P.uniform_fb = uniform_fallback;
     P.v = v; P.z = z; P.F = F; P.R = R; P.status = status;
+    P.valid = plan->d_valid;
     cudaStream_t st = (cudaStream_t)stream;
+    // which molecules the reduction covers, then the reduced kernels, then the
+    // elimination kernels for the rest (each pass draws from zeroed counters)
+    uneven_valid_kernel<<<(plan->n_mol + 127) / 128, 128, 0, st>>>(P, plan->n_mol, plan->d_valid);
+    if (mm_cuda_check(cudaGetLastError(), "uneven_valid_kernel launch")) return -3;
     if (mm_cuda_check(cudaMemsetAsync(plan->d_counter, 0, 3 * sizeof(int), st), "cudaMemsetAsync"))
         return -3;
-    int rc = launch_class<UC2>(P, plan, 2, persistent, st);
+    int rc = launch_class<UC2, true>(P, plan, 2, persistent, st);
+    if (!rc) rc = launch_class<UC1, true>(P, plan, 1, persistent, st);
+    if (!rc) rc = launch_class<UC0, true>(P, plan, 0, persistent, st);
+    if (!rc && mm_cuda_check(cudaMemsetAsync(plan->d_counter, 0, 3 * sizeof(int), st), "cudaMemsetAsync"))
+        return -3;
+    if (!rc) rc = launch_class<UC2>(P, plan, 2, persistent, st);
     if (!rc) rc = launch_class<UC1>(P, plan, 1, persistent, st);
     if (!rc) rc = launch_class<UC0>(P, plan, 0, persistent, st);
     return rc;
@@ -612,6 +764,7 @@ extern "C" int mm_uneven_force_static(const mm_bank *bank, const mm_beams *beams
     P.hbar = hbar > 0 ? hbar : MM_HBAR_JIT;
     P.uniform_fb = uniform_fallback;
     P.v = v; P.z = z; P.F = F; P.R = R; P.status = status;
+    P.valid = nullptr;  // the elimination kernels take every molecule
     int rc = launch_class<UC2>(P, &plan, 2, 1, st);
     if (!rc) rc = launch_class<UC1>(P, &plan, 1, 1, st);
     if (!rc) rc = launch_class<UC0>(P, &plan, 0, 1, st);
