@@ -69,6 +69,7 @@ struct Smem3 {
     double E[NGM + NEM], Ze[NEM];
     double khat[NBM][3], freq[NBM], s0[NBM], radius[NBM];
     int pol[NBM];
+    unsigned short sched[NGM - 1][NGM / 2];  // circle schedule: p | q << 8 of round r, slot i
     struct Group {
         double Hre[NGM * LDH], Him[NGM * LDH];
         double Vre[NGM * LDH], Vim[NGM * LDH];
@@ -90,6 +91,13 @@ __device__ __forceinline__ double gsum16(double x)
 }
 
 
+// Player at position j in round r of the circle schedule on NGM players:
+// position 0 stays, the others rotate; slot i pairs positions i and NGM-1-i.
+__host__ __device__ constexpr int rr_player(int r, int j)
+{
+    return j == 0 ? 0 : ((r + j - 1) % (NGM - 1)) + 1;
+}
+
 __device__ void load_consts3(const Force3Params &P, int set, Smem3 &S)
 {
     const int n_g = P.n_g, n_e = P.n_e, n_b = P.n_b, tid = threadIdx.x, nt = blockDim.x;
@@ -99,6 +107,10 @@ __device__ void load_consts3(const Force3Params &P, int set, Smem3 &S)
         S.Zim[a][rc] = P.Zim[i];
     }
     for (int i = tid; i < n_g * n_e * 3; i += nt) S.tdm[i] = P.tdm[i];
+    for (int i = tid; i < (NGM - 1) * (NGM / 2); i += nt) {
+        const int r = i / (NGM / 2), k = i % (NGM / 2);
+        S.sched[r][k] = (unsigned short)(rr_player(r, k) | rr_player(r, NGM - 1 - k) << 8);
+    }
     for (int i = tid; i < n_g + n_e; i += nt) S.E[i] = P.E[i];
     for (int i = tid; i < n_e; i += nt) S.Ze[i] = P.Ze[i];
     const size_t o = (size_t)set * n_b;
@@ -116,24 +128,19 @@ struct Out3 {
     int status;
 };
 
-// Player at position j in round r of the circle schedule on NGM players:
-// position 0 stays, the others rotate; slot i pairs positions i and NGM-1-i.
-__host__ __device__ constexpr int rr_player(int r, int j)
-{
-    return j == 0 ? 0 : ((r + j - 1) % (NGM - 1)) + 1;
-}
 
 // One round of NGM/2 disjoint complex Jacobi rotations (H <- J^H H J,
-// V <- V J, J = [[c, s], [-conj(s), c]] on columns p, q).  Lanes 0..NGM/2-1
-// compute the rotations; then lane t updates row t of H and V (columns p, q of
-// every pair) and column t of H (rows p, q).  Every index is a compile-time
-// constant except t.
-template <int RND>
-__device__ __forceinline__ void jacobi_round(Smem3::Group &W, int t)
+// V <- V J, J = [[c, s], [-conj(s), c]] on columns p, q).  pq[i] holds the
+// players of slot i of this round (p | q << 8).  Lanes 0..NGM/2-1 compute the
+// rotations; then lane t updates row t of H and V (columns p, q of every
+// pair) and column t of H (rows p, q).  The round index is a run-time value
+// (one copy of this code serves the NGM - 1 rounds); the pair loop is
+// unrolled.
+__device__ __forceinline__ void jacobi_round(Smem3::Group &W, int t, const unsigned short *pq)
 {
     constexpr int NP = NGM / 2;
     if (t < NP) {
-        const int p = rr_player(RND, t), q = rr_player(RND, NGM - 1 - t);
+        const int p = pq[t] & 0xff, q = pq[t] >> 8;
         double c = 1.0, sr = 0.0, si = 0.0;
         const double a = W.Hre[p * LDH + p], b = W.Hre[q * LDH + q];
         const double xr = W.Hre[p * LDH + q], xi = W.Him[p * LDH + q];
@@ -156,28 +163,27 @@ __device__ __forceinline__ void jacobi_round(Smem3::Group &W, int t)
     __syncwarp();
     if (t < NGM) {
         // columns p, q of H and V in row t:  a_p' = a_p c - a_q conj(s);  a_q' = a_p s + a_q c
-        static_for<0, NP>([&](auto ic) {
-            constexpr int i = decltype(ic)::value;
-            constexpr int p = rr_player(RND, i), q = rr_player(RND, NGM - 1 - i);
+#pragma unroll
+        for (int i = 0; i < NP; i++) {
+            const int p = pq[i] & 0xff, q = pq[i] >> 8;
             const double c = W.rot[i][0], sr = W.rot[i][1], si = W.rot[i][2];
-            double *Xr = W.Hre + t * LDH, *Xi = W.Him + t * LDH;
+#pragma unroll
             for (int m = 0; m < 2; m++) {
+                double *Xr = (m ? W.Vre : W.Hre) + t * LDH, *Xi = (m ? W.Vim : W.Him) + t * LDH;
                 const double apr = Xr[p], api = Xi[p], aqr = Xr[q], aqi = Xi[q];
                 Xr[p] = apr * c - (aqr * sr + aqi * si);
                 Xi[p] = api * c - (aqi * sr - aqr * si);
                 Xr[q] = (apr * sr - api * si) + aqr * c;
                 Xi[q] = (apr * si + api * sr) + aqi * c;
-                Xr = W.Vre + t * LDH;
-                Xi = W.Vim + t * LDH;
             }
-        });
+        }
     }
     __syncwarp();
     if (t < NGM) {
         // rows p, q of H in column t:  a_p' = c a_p - s a_q;  a_q' = conj(s) a_p + c a_q
-        static_for<0, NP>([&](auto ic) {
-            constexpr int i = decltype(ic)::value;
-            constexpr int p = rr_player(RND, i), q = rr_player(RND, NGM - 1 - i);
+#pragma unroll
+        for (int i = 0; i < NP; i++) {
+            const int p = pq[i] & 0xff, q = pq[i] >> 8;
             const double c = W.rot[i][0], sr = W.rot[i][1], si = W.rot[i][2];
             const double apr = W.Hre[p * LDH + t], api = W.Him[p * LDH + t];
             const double aqr = W.Hre[q * LDH + t], aqi = W.Him[q * LDH + t];
@@ -185,11 +191,11 @@ __device__ __forceinline__ void jacobi_round(Smem3::Group &W, int t)
             W.Him[p * LDH + t] = c * api - (sr * aqi + si * aqr);
             W.Hre[q * LDH + t] = (sr * apr + si * api) + c * aqr;
             W.Him[q * LDH + t] = (sr * api - si * apr) + c * aqi;
-        });
+        }
     }
     __syncwarp();
     if (t < NP) {  // exact zero of the rotated pair, real diagonal
-        const int p = rr_player(RND, t), q = rr_player(RND, NGM - 1 - t);
+        const int p = pq[t] & 0xff, q = pq[t] >> 8;
         if (W.rot[t][1] != 0.0 || W.rot[t][2] != 0.0) {
             W.Hre[p * LDH + q] = 0.0; W.Him[p * LDH + q] = 0.0;
             W.Hre[q * LDH + p] = 0.0; W.Him[q * LDH + p] = 0.0;
@@ -255,7 +261,8 @@ __device__ Out3 force3d_point(const Force3Params &P, Smem3 &S, Smem3::Group &W, 
         dia = gsum16(dia);
         const bool more = off > 1e-30 * dia && off > 1e-300;
         if (!__any_sync(FULL, more)) break;
-        static_for<0, NGM - 1>([&](auto rc) { jacobi_round<decltype(rc)::value>(W, t); });
+#pragma unroll 1
+        for (int rnd = 0; rnd < NGM - 1; rnd++) jacobi_round(W, t, S.sched[rnd]);
     }
     // ascending order (ties by index), as eigh returns the spectrum
     if (t < n_g) {
