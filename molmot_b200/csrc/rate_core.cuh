@@ -129,11 +129,14 @@ struct SmemLayout {
         cnt = o; o = al(o + sizeof(int) * n_g);
         off = o; o = al(o + sizeof(int) * n_g);
         maxcnt = o; o = al(o + sizeof(int) * cpl);
-        ntrip_max = n_g * n_b * n_e;
+        // + 3 n_g: each ground state's list starts at an offset = k (mod 4), so
+        // the 4 lanes of a group read records in different banks
+        ntrip_max = n_g * n_b * n_e + 3 * n_g;
         trip = o; o = al(o + (fp32 ? sizeof(Trip32) : sizeof(Trip64)) * (size_t)ntrip_max);
         d2t = o; o = al(o + sizeof(double) * (size_t)(fp32 ? 0 : ntrip_max));
         // FP64 form: doppler-shifted frequencies, excited energies, adjoint accumulators
-        scratch_per_group = fp32 ? 0 : n_b + n_e + 2 * n_b;
+        // a stride of 2 (mod 4) doubles puts the 8 groups of a warp in distinct banks
+        scratch_per_group = fp32 ? 0 : ((n_b + n_e + 2 * n_b + 1) / 4) * 4 + 2;
         scratch = o; o = al(o + sizeof(double) * (size_t)scratch_per_group * ngroups);
         total = o;
     }
@@ -178,7 +181,11 @@ __device__ void build_set_tables(const ForceParams &P, int set, unsigned char *s
     __syncthreads();
     if (tid == 0) {
         int o = 0;
-        for (int k = 0; k < n_g; k++) { off[k] = o; o += cnt[k]; }
+        for (int k = 0; k < n_g; k++) {
+            o += (k - o) & 3;  // o = k (mod 4): the lanes of a group read different banks
+            off[k] = o;
+            o += cnt[k];
+        }
         for (int c = 0; c < CPL; c++) {
             int m = 0;
             for (int t = 0; t < G; t++) {

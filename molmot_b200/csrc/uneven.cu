@@ -85,8 +85,12 @@ struct ULayout {
     // per group
     // elimination: A, Rm, bv, xv, invU, Fk, Rk, Esg, fd, Ese
     // reduced:     Rm (scaled rates), K, Fk, Rk, Esg, w, phi, fd, Ese, cw, cf, rs, pi
-    static constexpr int grp_doubles = RED ? NGMAX * NEMAX + NEMAX * LDK + 5 * NGMAX + NBU + 5 * NEMAX
-                                           : NGMAX * LDA + NGMAX * NEMAX + 6 * NGMAX + NBU + NEMAX;
+    static constexpr int grp_raw = RED ? NGMAX * NEMAX + NEMAX * LDK + 5 * NGMAX + NBU + 5 * NEMAX
+                                       : NGMAX * LDA + NGMAX * NEMAX + 6 * NGMAX + NBU + NEMAX;
+    // two 16-lane groups of a warp read the same offsets of their own region:
+    // a stride of 16 banks past a multiple of 128 bytes keeps those reads
+    // conflict-free (a multiple of 128 bytes would put both in the same banks)
+    static constexpr int grp_doubles = (grp_raw + 15) / 16 * 16 + 8;
     static size_t bytes(int groups)
     {
         return sizeof(double) * (size_t)(mol_doubles + beam_doubles + groups * grp_doubles) +
