@@ -146,3 +146,14 @@ def make_position_sampler(sigma=1e-3, method="gaussian"):
     if method == "uniform_sphere":
         return lambda: sample_uniform_sphere(sigma, 1, rng)
     raise ValueError(f"Unknown method: {method}")
+
+
+def make_velocity_sampler(temperature, mass, method="maxwell_boltzmann"):
+    """Callable returning one 3D velocity per call: Maxwell-Boltzmann at
+    `temperature`, or zero ('fixed') (molmot/propagation/trajectories.py:413-446)."""
+    rng = np.random.default_rng()
+    if method == "maxwell_boltzmann":
+        return lambda: sample_maxwell_boltzmann(temperature, mass, 1, rng)
+    if method == "fixed":
+        return lambda: np.zeros(3)
+    raise ValueError(f"Unknown method: {method}")

@@ -46,6 +46,14 @@ def test_samplers_moments():
     assert np.all(np.abs(d.mean(0)) < 0.1)
     u = tr.sample_uniform_sphere(2e-3, 500, rng)
     assert np.all(np.linalg.norm(u, axis=1) <= 2e-3)
+    vs = tr.make_velocity_sampler(5e-3, 1.74356601993e-25)
+    vv = np.array([vs() for _ in range(4000)])
+    assert vv.shape == (4000, 3) and abs(vv.std() / sigma - 1) < 0.1
+    assert np.array_equal(tr.make_velocity_sampler(5e-3, 1.0, "fixed")(), np.zeros(3))
+    ps = tr.make_position_sampler(1e-3, "uniform_sphere")
+    assert np.linalg.norm(ps()) <= 1e-3
+    with pytest.raises(ValueError):
+        tr.make_velocity_sampler(5e-3, 1.0, "thermal")
 
 
 def test_as_gpu_simulator_rejects_unknown():
