@@ -192,26 +192,36 @@ uneven_kernel(UnevenParams P)
             // rates of ground states k = t, t + G, ... (rows of Rm owned by this lane)
             for (int k = t; k < n_g; k += G) {
                 double s = 0.0, f = 0.0;
-                for (int e = 0; e < n_e; e++) Rm[k * NEMAX + e] = 0.0;
+                double Racc[NEMAX];  // per excited state, in registers (compile-time index)
+#pragma unroll
+                for (int e = 0; e < NEMAX; e++) Racc[e] = 0.0;
+                const double Eg = Esg[k];
                 for (int b = 0; b < n_b; b++) {
                     const int q = pol[b];
-                    for (int e = 0; e < n_e; e++) {
+                    const double fdb = fd[b], c1b = c1[b], hkb = hk[b], s0b = s0[b];
+#pragma unroll
+                    for (int e = 0; e < NEMAX; e++) {
+                        if (e >= n_e) break;
                         const double d2 = d2s[(k * n_e + e) * 3 + q];
                         if (d2 < 1e-15) continue;
-                        const double om = __dsub_rn(Ese[e], Esg[k]);
-                        const double de = __dmul_rn(__dsub_rn(fd[b], om), MM_TWO_PI);
+                        const double om = __dsub_rn(Ese[e], Eg);
+                        const double de = __dmul_rn(__dsub_rn(fdb, om), MM_TWO_PI);
                         const double L = gh2 * mm_rcp(fma(de, de, gh2));
-                        const double ru = c1[b] * d2 * P.geff * L;
-                        Rm[k * NEMAX + e] += ru;
-                        f = fma(hk[b], ru, f);
-                        s = fma(s0[b] * d2, L, s);
+                        const double ru = c1b * d2 * P.geff * L;
+                        Racc[e] += ru;
+                        f = fma(hkb, ru, f);
+                        s = fma(s0b * d2, L, s);
                     }
                 }
                 const double sat = mm_rcp(1.0 + s);
                 double rs = 0.0;
-                for (int e = 0; e < n_e; e++) {
-                    Rm[k * NEMAX + e] *= sat;
-                    rs += Rm[k * NEMAX + e];
+#pragma unroll
+                for (int e = 0; e < NEMAX; e++) {
+                    if (e < n_e) {
+                        const double r = Racc[e] * sat;
+                        Rm[k * NEMAX + e] = r;
+                        rs += r;
+                    }
                 }
                 Fk[k] = f * sat;
                 Rk[k] = rs;
