@@ -35,7 +35,6 @@ constexpr int NGM = 12;        // max ground states of the 3D kernel (SrOH-sized
 constexpr int NEM = 4;         // max excited states
 constexpr int NBM = 32;        // max beams
 constexpr int LDH = NGM + 1;   // padded row length of the matrices in shared memory
-constexpr int DSQ_LD = NEM * 3 + 1;  // odd row length: lane rows fall in distinct banks
 
 struct Force3Params {
     int n_g, n_e, n_b, n_sets;
@@ -77,11 +76,11 @@ struct Smem3 {
         double rot[NGM / 2][3];      // c, Re s, Im s
         double lam[NGM];
         int perm[NGM];
-        double dsq[NGM * DSQ_LD];    // row a: |U^H d|^2 of eigenstate a, [e][q], padded row
+        double dsq[NEM * 3 * NGM];   // |U^H d|^2 at [(e * 3 + q) * NGM + a]: lanes a read consecutive doubles
         double BR[NEM * NGM];
         double Esg[NGM], Ese[NEM];
         double bm[NBM][5];           // doppler, s_eff, w0, w1, w2
-        double pad_[8];              // see the size check below
+        double pad_[4];              // see the size check below
     } grp[kThreads3 / kG3];
 };
 
@@ -302,7 +301,7 @@ __device__ Out3 force3d_point(const Force3Params &P, Smem3 &S, Smem3::Group &W, 
                     ai -= W.Vim[g * LDH + col] * d;
                 }
                 const double d2 = ar * ar + ai * ai;
-                W.dsq[t * DSQ_LD + e * 3 + q] = d2;
+                W.dsq[(e * 3 + q) * NGM + t] = d2;
                 rowsum[e] += d2;
             }
         }
@@ -362,7 +361,7 @@ __device__ Out3 force3d_point(const Force3Params &P, Smem3 &S, Smem3::Group &W, 
                     double ws = 0.0;
 #pragma unroll
                     for (int q = 0; q < 3; q++) {
-                        const double d2 = W.dsq[t * DSQ_LD + e * 3 + q];
+                        const double d2 = W.dsq[(e * 3 + q) * NGM + t];
                         if (d2 >= 1e-15) ws = fma(W.bm[b][2 + q], d2, ws);
                     }
                     const double rb = ws * L * se;
