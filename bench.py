@@ -432,7 +432,7 @@ def main():
 
     A = active_triples(mol.d_squared, pol[0])
     f64_32, f32_32 = flops_reduced(12, 4, A)
-    f64_64, _ = flops_per_point(12, 4, 8, A, refine=False)
+    f64_64, _ = flops_per_point(12, 4, 8, A)
     # FP32 form: FP64 and FP32 pipes run concurrently; the bound is the slower of the two
     t_min32 = max(f64_32 * n_pts / (peaks["fp64"] * 1e12), f32_32 * n_pts / (peaks["fp32"] * 1e12))
     achieved32 = (f64_32 + f32_32) * n_pts / (ms32 * 1e-3) / 1e12

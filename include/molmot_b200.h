@@ -38,9 +38,9 @@ extern "C" {
 
 /* precision of the force kernels */
 #define MM_PREC_FP64 0         /* plain FP64, reference operation order */
-#define MM_PREC_FP32_REFINE 1  /* FP32-bulk: FP32 Lorentzians with FP64 sums; force batches solve
-                                  the populations in FP64 through the excited-state chain
-                                  (reduced.cuh), trajectories by FP64 LU + 1 refinement step */
+#define MM_PREC_FP32_REFINE 1  /* FP32-bulk: FP32 Lorentzians with FP64 sums, populations in FP64
+                                  through the excited-state chain (reduced.cuh), one point or
+                                  particle per thread (the name is kept for the ABI) */
 #define MM_PREC_FP64_REDUCED 2 /* mm_force_batch only: FP64 rates in the plain form's operation order,
                                   populations from the same FP64 excited-chain solve as
                                   MM_PREC_FP32_REFINE (agrees with MM_PREC_FP64 to rounding) */

@@ -15,7 +15,7 @@ namespace {
 
 constexpr int kThreads = 128;
 
-template <int NGMAX, int NEMAX, int G, bool FP32, bool EXACT>
+template <int NGMAX, int NEMAX, int G, bool EXACT>
 __global__ void __launch_bounds__(kThreads, 3)
 force_kernel(ForceParams P)
 {
@@ -23,7 +23,7 @@ force_kernel(ForceParams P)
     extern __shared__ __align__(16) unsigned char sm[];
     SmemLayout Ly;
     const int ngroups = kThreads / G;
-    Ly.build(P.n_g, P.n_e, P.n_b, GS::CPL, ngroups, FP32);
+    Ly.build(P.n_g, P.n_e, P.n_b, GS::CPL, ngroups);
     const long long pts_per_set = (P.layout == MM_LAYOUT_GRID) ? P.nv * P.nz : P.pps;
 
     const int lane = threadIdx.x & 31, t = lane % G, gbase = lane - t;
@@ -38,7 +38,7 @@ force_kernel(ForceParams P)
         if (set_count <= 0) continue;  // uniform over the CTA
         SetView S;
         __syncthreads();
-        build_set_tables<G, GS::CPL, FP32>(P, set, sm, Ly, S);
+        build_set_tables<G, GS::CPL>(P, set, sm, Ly, S);
         const double Bg = P.bgrad[set];
         const long long chunk = (set_count + gridDim.x - 1) / gridDim.x;
         const long long start = (long long)blockIdx.x * chunk;
@@ -56,8 +56,7 @@ force_kernel(ForceParams P)
                 z = P.z[set_first + ipc];
             }
             double xs[GS::CPL];
-            const PointOut o = solve_point<NGMAX, NEMAX, G, FP32, EXACT>(P, S, fd, Ese, t, gbase, v, z,
-                                                                          Bg, xs);
+            const PointOut o = solve_point<NGMAX, NEMAX, G, EXACT>(P, S, fd, Ese, t, gbase, v, z, Bg, xs);
             if (valid) {
                 const long long gi = set_first + ip;
                 if (t == 0) {
@@ -89,7 +88,7 @@ force_adjoint_kernel(ForceParams P, double *grad)
     extern __shared__ __align__(16) unsigned char sm[];
     SmemLayout Ly;
     const int ngroups = kThreads / G;
-    Ly.build(P.n_g, P.n_e, P.n_b, GS::CPL, ngroups, false);
+    Ly.build(P.n_g, P.n_e, P.n_b, GS::CPL, ngroups);
     const long long pts_per_set = (P.layout == MM_LAYOUT_GRID) ? P.nv * P.nz : P.pps;
     const int lane = threadIdx.x & 31, t = lane % G, gbase = lane - t;
     const int group = threadIdx.x / G;
@@ -103,7 +102,7 @@ force_adjoint_kernel(ForceParams P, double *grad)
         if (set_count <= 0) continue;
         SetView S;
         __syncthreads();
-        build_set_tables<G, GS::CPL, false>(P, set, sm, Ly, S);
+        build_set_tables<G, GS::CPL>(P, set, sm, Ly, S);
         const double Bg = P.bgrad[set];
         const long long chunk = (set_count + gridDim.x - 1) / gridDim.x;
         const long long start = (long long)blockIdx.x * chunk;
@@ -121,7 +120,7 @@ force_adjoint_kernel(ForceParams P, double *grad)
                 z = P.z[set_first + ipc];
             }
             double xs[GS::CPL];
-            const PointOut o = solve_point<NGMAX, NEMAX, G, false, EXACT, true>(
+            const PointOut o = solve_point<NGMAX, NEMAX, G, EXACT, true>(
                 P, S, fd, Ese, t, gbase, v, z, Bg, xs, gacc);
             if (valid) {
                 const long long gi = set_first + ip;
@@ -225,7 +224,7 @@ struct TrajParams {
 //            (molmot/propagation/trajectories.py:159-229, monte_carlo_temperature).
 // The integrator uses explicit round-to-nearest operations so it matches the
 // reference's uncontracted arithmetic.
-template <int NGMAX, int NEMAX, int G, bool FP32, bool EXACT>
+template <int NGMAX, int NEMAX, int G, bool EXACT>
 __global__ void __launch_bounds__(kThreads, 3)
 traj1d_kernel(ForceParams P, TrajParams T)
 {
@@ -233,7 +232,7 @@ traj1d_kernel(ForceParams P, TrajParams T)
     extern __shared__ __align__(16) unsigned char sm[];
     SmemLayout Ly;
     const int ngroups = kThreads / G;
-    Ly.build(P.n_g, P.n_e, P.n_b, GS::CPL, ngroups, FP32);
+    Ly.build(P.n_g, P.n_e, P.n_b, GS::CPL, ngroups);
     const int lane = threadIdx.x & 31, t = lane % G, gbase = lane - t;
     const int group = threadIdx.x / G;
     double *scr = (double *)(sm + Ly.scratch) + (size_t)group * Ly.scratch_per_group;
@@ -241,7 +240,7 @@ traj1d_kernel(ForceParams P, TrajParams T)
     SetView S[2];
     double Bg[2];
     for (int a = 0; a < T.n_avg; a++) {
-        build_set_tables<G, GS::CPL, FP32>(P, a, sm + a * Ly.total, Ly, S[a]);
+        build_set_tables<G, GS::CPL>(P, a, sm + a * Ly.total, Ly, S[a]);
         Bg[a] = P.bgrad[a];
     }
     const int nd = T.ndim;
@@ -267,7 +266,7 @@ traj1d_kernel(ForceParams P, TrajParams T)
             double F = 0.0;
             for (int a = 0; a < T.n_avg; a++) {
                 double xs[GS::CPL];
-                const PointOut o = solve_point<NGMAX, NEMAX, G, FP32, EXACT>(
+                const PointOut o = solve_point<NGMAX, NEMAX, G, EXACT>(
                     P, S[a], fd, Ese, t, gbase, u[d], x[d], Bg[a] * mult, xs);
                 F = (a == 0) ? o.F : __dadd_rn(F, o.F);
             }
@@ -391,19 +390,19 @@ struct Class {
     static constexpr bool exact = EXACT;
 };
 
-template <class C, bool FP32>
+template <class C>
 size_t smem_bytes(const ForceParams &P)
 {
     SmemLayout Ly;
-    Ly.build(P.n_g, P.n_e, P.n_b, GroupShape<C::ng, C::ne, C::g>::CPL, kThreads / C::g, FP32);
+    Ly.build(P.n_g, P.n_e, P.n_b, GroupShape<C::ng, C::ne, C::g>::CPL, kThreads / C::g);
     return Ly.total;
 }
 
-template <class C, bool FP32>
+template <class C>
 int launch_force(const ForceParams &P, long long pts_per_set, cudaStream_t st)
 {
-    auto kern = force_kernel<C::ng, C::ne, C::g, FP32, C::exact>;
-    const size_t sb = smem_bytes<C, FP32>(P);
+    auto kern = force_kernel<C::ng, C::ne, C::g, C::exact>;
+    const size_t sb = smem_bytes<C>(P);
     if (sb > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb);
         if (mm_cuda_check(e, "cudaFuncSetAttribute")) return -3;
@@ -474,7 +473,7 @@ template <class C>
 int launch_adjoint(const ForceParams &P, double *grad, cudaStream_t st)
 {
     auto kern = force_adjoint_kernel<C::ng, C::ne, C::g, C::exact>;
-    const size_t sb = smem_bytes<C, false>(P);
+    const size_t sb = smem_bytes<C>(P);
     if (sb > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb);
         if (mm_cuda_check(e, "cudaFuncSetAttribute")) return -3;
@@ -494,11 +493,11 @@ int launch_adjoint(const ForceParams &P, double *grad, cudaStream_t st)
     return mm_cuda_check(cudaGetLastError(), "force_adjoint_kernel launch") ? -3 : 0;
 }
 
-template <class C, bool FP32>
+template <class C>
 int launch_traj(const ForceParams &P, const TrajParams &T, cudaStream_t st)
 {
-    auto kern = traj1d_kernel<C::ng, C::ne, C::g, FP32, C::exact>;
-    const size_t sb = smem_bytes<C, FP32>(P) * T.n_avg;
+    auto kern = traj1d_kernel<C::ng, C::ne, C::g, C::exact>;
+    const size_t sb = smem_bytes<C>(P) * T.n_avg;
     if (sb > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb);
         if (mm_cuda_check(e, "cudaFuncSetAttribute")) return -3;
@@ -639,7 +638,7 @@ extern "C" int mm_force_batch(const mm_pack *pack, const mm_beams *beams, const 
     cudaStream_t st = (cudaStream_t)stream;
     return dispatch_class(P.n_g, P.n_e, [&](auto C) -> int {
         using CT = decltype(C);
-        if (prec == MM_PREC_FP64) return launch_force<CT, false>(P, pps, st);
+        if (prec == MM_PREC_FP64) return launch_force<CT>(P, pps, st);
         const bool pad = reduced_list_granule(pack, beams) == kRedPad;
         if (prec == MM_PREC_FP64_REDUCED)
             return pad ? launch_reduced<CT, kRedPad, true>(P, pps, st) : launch_reduced<CT, 1, true>(P, pps, st);
@@ -688,7 +687,7 @@ extern "C" int mm_traj_run(const mm_pack *pack, const mm_beams *beams, const mm_
     cudaStream_t st = (cudaStream_t)stream;
     return dispatch_class(P.n_g, P.n_e, [&](auto C) -> int {
         using CT = decltype(C);
-        if (!fp32) return launch_traj<CT, false>(P, T, st);
+        if (!fp32) return launch_traj<CT>(P, T, st);
         return reduced_list_granule(pack, beams) == kRedPad ? launch_traj_reduced<CT, kRedPad>(P, T, st)
                                                             : launch_traj_reduced<CT, 1>(P, T, st);
     });

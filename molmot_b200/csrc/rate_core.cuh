@@ -88,16 +88,6 @@ struct Trip64 {
     int be;      // b | e << 8
     int pad;
 };
-struct Trip32 {
-    float d0;    // freq_b - (E_e - E_g), FP64 then rounded  (Hz)
-    float dzd;   // (zd_e - zd_g) Gamma / (2 pi)              (Hz per G)
-    float kdf;   // -k kdir_b / (2 pi)                        (Hz per m/s)
-    float c1g;   // (Gamma/2) s0 d2 Geff
-    float c2;    // s0 d2
-    float hkf;   // hbar k kdir_b
-    int be;
-    int pad;
-};
 
 // Shared-memory view of one parameter set's tables.
 struct SetView {
@@ -105,7 +95,6 @@ struct SetView {
     const double *freq, *ck;          // per beam: freq, (-k) kdir
     const int *cnt, *off, *maxcnt;    // per ground state / per slot
     const Trip64 *t64;
-    const Trip32 *t32;
     const double *d2t;                // |d|^2 of each FP64 triple (adjoint)
 };
 
@@ -116,7 +105,7 @@ struct SmemLayout {
 
     __host__ __device__ static size_t al(size_t x) { return (x + 15) & ~size_t(15); }
 
-    __host__ __device__ void build(int n_g, int n_e, int n_b, int cpl, int ngroups, bool fp32)
+    __host__ __device__ void build(int n_g, int n_e, int n_b, int cpl, int ngroups)
     {
         const int n_s = n_g + n_e;
         size_t o = 0;
@@ -132,18 +121,18 @@ struct SmemLayout {
         // + 3 n_g: each ground state's list starts at an offset = k (mod 4), so
         // the 4 lanes of a group read records in different banks
         ntrip_max = n_g * n_b * n_e + 3 * n_g;
-        trip = o; o = al(o + (fp32 ? sizeof(Trip32) : sizeof(Trip64)) * (size_t)ntrip_max);
-        d2t = o; o = al(o + sizeof(double) * (size_t)(fp32 ? 0 : ntrip_max));
-        // FP64 form: doppler-shifted frequencies, excited energies, adjoint accumulators
+        trip = o; o = al(o + sizeof(Trip64) * (size_t)ntrip_max);
+        d2t = o; o = al(o + sizeof(double) * (size_t)ntrip_max);
+        // doppler-shifted frequencies, excited energies, adjoint accumulators
         // a stride of 2 (mod 4) doubles puts the 8 groups of a warp in distinct banks
-        scratch_per_group = fp32 ? 0 : ((n_b + n_e + 2 * n_b + 1) / 4) * 4 + 2;
+        scratch_per_group = ((n_b + n_e + 2 * n_b + 1) / 4) * 4 + 2;
         scratch = o; o = al(o + sizeof(double) * (size_t)scratch_per_group * ngroups);
         total = o;
     }
 };
 
 // Build the parameter-set tables (all threads of the CTA participate).
-template <int G, int CPL, bool FP32>
+template <int G, int CPL>
 __device__ void build_set_tables(const ForceParams &P, int set, unsigned char *sm,
                                  const SmemLayout &Ly, SetView &S)
 {
@@ -153,7 +142,6 @@ __device__ void build_set_tables(const ForceParams &P, int set, unsigned char *s
     double *freq = (double *)(sm + Ly.freq), *ck = (double *)(sm + Ly.ck);
     int *cnt = (int *)(sm + Ly.cnt), *off = (int *)(sm + Ly.off), *maxcnt = (int *)(sm + Ly.maxcnt);
     Trip64 *t64 = (Trip64 *)(sm + Ly.trip);
-    Trip32 *t32 = (Trip32 *)(sm + Ly.trip);
     double *d2t = (double *)(sm + Ly.d2t);
     const int tid = threadIdx.x, nt = blockDim.x;
     const double *kdir = P.kdir + (size_t)set * n_b, *fr = P.freq + (size_t)set * n_b;
@@ -206,32 +194,19 @@ __device__ void build_set_tables(const ForceParams &P, int set, unsigned char *s
                 if (d2 < 1e-15) continue;
                 const double c1 = __dmul_rn(__dmul_rn(gh, s0[b]), d2);
                 const double hk = __dmul_rn(__dmul_rn(P.hbar, P.k), kdir[b]);
-                if (!FP32) {
-                    Trip64 tr;
-                    tr.c1g = c1 * P.geff;
-                    tr.c2 = __dmul_rn(s0[b], d2);
-                    tr.hk = hk;
-                    tr.be = b | (e << 8);
-                    tr.pad = 0;
-                    d2t[o] = d2;
-                    t64[o++] = tr;
-                } else {
-                    Trip32 tr;
-                    tr.d0 = (float)(fr[b] - (P.E[n_g + e] - P.E[k]));
-                    tr.dzd = (float)((P.zd[n_g + e] - P.zd[k]) * P.Gamma / MM_TWO_PI);
-                    tr.kdf = (float)(ck[b] / MM_TWO_PI);
-                    tr.c1g = (float)(c1 * P.geff);
-                    tr.c2 = (float)(s0[b] * d2);
-                    tr.hkf = (float)hk;
-                    tr.be = b | (e << 8);
-                    tr.pad = 0;
-                    t32[o++] = tr;
-                }
+                Trip64 tr;
+                tr.c1g = c1 * P.geff;
+                tr.c2 = __dmul_rn(s0[b], d2);
+                tr.hk = hk;
+                tr.be = b | (e << 8);
+                tr.pad = 0;
+                d2t[o] = d2;
+                t64[o++] = tr;
             }
     }
     __syncthreads();
     S.E = E; S.zd = zd; S.czd = czd; S.BR = BR; S.freq = freq; S.ck = ck;
-    S.cnt = cnt; S.off = off; S.maxcnt = maxcnt; S.t64 = t64; S.t32 = t32; S.d2t = d2t;
+    S.cnt = cnt; S.off = off; S.maxcnt = maxcnt; S.t64 = t64; S.d2t = d2t;
 }
 
 // Result of one point, identical in every lane of the group.
@@ -250,7 +225,7 @@ struct GroupShape {
 // fd / Ese: this group's scratch (n_b + n_e doubles) in shared memory
 // (FP64 form only).  EXACT: the molecule has exactly NGMAX ground and NEMAX
 // excited states (size predicates vanish at compile time).
-template <int NGMAX, int NEMAX, int G, bool FP32, bool EXACT, bool ADJ = false>
+template <int NGMAX, int NEMAX, int G, bool EXACT, bool ADJ = false>
 __device__ __forceinline__ PointOut solve_point(const ForceParams &P, const SetView &S, double *fd,
                                                 double *Ese, int t, int gbase, double v, double z,
                                                 double Bgrad,
@@ -269,19 +244,16 @@ __device__ __forceinline__ PointOut solve_point(const ForceParams &P, const SetV
     double R[CPL][NEMAX];
     double Fk[CPL], Rk[CPL], satk[CPL];
     const double B_gauss = __dmul_rn(__dmul_rn(Bgrad, z), 1e4);
-    if (!FP32) {
-        __syncwarp();
-        // laser frequency seen by the moving molecule, per beam (exact order)
-        for (int b = t; b < P.n_b; b += G)
-            fd[b] = __dadd_rn(S.freq[b], __ddiv_rn(__dmul_rn(S.ck[b], v), MM_TWO_PI));
-        // Zeeman-shifted excited energies (exact order)
-        for (int e = t; e < n_e; e += G)
-            Ese[e] = __dadd_rn(S.E[n_g + e], __ddiv_rn(__dmul_rn(__dmul_rn(B_gauss, S.zd[n_g + e]),
-                                                                 P.Gamma), MM_TWO_PI));
-        __syncwarp();
-    }
-    const float Bf = (float)B_gauss, vf = (float)v;
-    const float cu = (float)(MM_TWO_PI / gh);  // u = delta/(Gamma/2) = x * 2 pi/(Gamma/2)
+    __syncwarp();
+    // laser frequency seen by the moving molecule, per beam (exact order)
+    for (int b = t; b < P.n_b; b += G)
+        fd[b] = __dadd_rn(S.freq[b], __ddiv_rn(__dmul_rn(S.ck[b], v), MM_TWO_PI));
+    // Zeeman-shifted excited energies (exact order)
+    for (int e = t; e < n_e; e += G)
+        Ese[e] = __dadd_rn(S.E[n_g + e], __ddiv_rn(__dmul_rn(__dmul_rn(B_gauss, S.zd[n_g + e]),
+                                                             P.Gamma), MM_TWO_PI));
+    __syncwarp();
+
 #pragma unroll
     for (int c = 0; c < CPL; c++) {
         const int k = c * G + t;
@@ -290,73 +262,39 @@ __device__ __forceinline__ PointOut solve_point(const ForceParams &P, const SetV
         const int cntk = own ? S.cnt[kk] : 0;
         const int o = S.off[kk];
         const int mc = S.maxcnt[c];
-        if (!FP32) {
-            double Rr[NEMAX];
+        double Rr[NEMAX];
 #pragma unroll
-            for (int e = 0; e < NEMAX; e++) Rr[e] = 0.0;
-            // ground-state shift: |error| <= 1 ulp of E_g (1.5e10 Hz), i.e. 2e-6 Hz
-            const double Esg = fma(B_gauss, S.czd[kk], S.E[kk]);
-            double s = 0.0, f = 0.0;
+        for (int e = 0; e < NEMAX; e++) Rr[e] = 0.0;
+        // ground-state shift: |error| <= 1 ulp of E_g (1.5e10 Hz), i.e. 2e-6 Hz
+        const double Esg = fma(B_gauss, S.czd[kk], S.E[kk]);
+        double s = 0.0, f = 0.0;
 #pragma unroll 2
-            for (int i = 0; i < mc; i++) {
-                if (i < cntk) {
-                    const Trip64 tr = S.t64[o + i];
-                    const int b = tr.be & 0xff, e = tr.be >> 8;
-                    const double om = __dsub_rn(Ese[e], Esg);
-                    const double de = __dmul_rn(__dsub_rn(fd[b], om), MM_TWO_PI);
-                    const double L = gh2 * mm_rcp(fma(de, de, gh2));
-                    const double ru = tr.c1g * L;
+        for (int i = 0; i < mc; i++) {
+            if (i < cntk) {
+                const Trip64 tr = S.t64[o + i];
+                const int b = tr.be & 0xff, e = tr.be >> 8;
+                const double om = __dsub_rn(Ese[e], Esg);
+                const double de = __dmul_rn(__dsub_rn(fd[b], om), MM_TWO_PI);
+                const double L = gh2 * mm_rcp(fma(de, de, gh2));
+                const double ru = tr.c1g * L;
 #pragma unroll
-                    for (int ee = 0; ee < NEMAX; ee++)
-                        if (ee == e) Rr[ee] += ru;
-                    f = fma(tr.hk, ru, f);
-                    s = fma(tr.c2, L, s);
-                }
+                for (int ee = 0; ee < NEMAX; ee++)
+                    if (ee == e) Rr[ee] += ru;
+                f = fma(tr.hk, ru, f);
+                s = fma(tr.c2, L, s);
             }
-            // saturation correction 1/(1 + s_total[g]) (rate_equations_jit.py:85-90)
-            const double sat = mm_rcp(1.0 + s);
-            satk[c] = sat;
-            double rs = 0.0;
-#pragma unroll
-            for (int e = 0; e < NEMAX; e++) {
-                R[c][e] = Rr[e] * sat;
-                rs += R[c][e];
-            }
-            Rk[c] = rs;
-            Fk[c] = f * sat;
-        } else {
-            // FP32 bulk: delta/2pi = d0 + kdf v - B dzd, all in FP32 (d0 from FP64)
-            float Rf[NEMAX];
-#pragma unroll
-            for (int e = 0; e < NEMAX; e++) Rf[e] = 0.f;
-            float s = 0.f, f = 0.f;
-#pragma unroll 2
-            for (int i = 0; i < mc; i++) {
-                if (i < cntk) {
-                    const Trip32 tr = S.t32[o + i];
-                    const int e = tr.be >> 8;
-                    float x = fmaf(tr.kdf, vf, tr.d0);
-                    x = fmaf(-Bf, tr.dzd, x);
-                    const float u = x * cu;
-                    const float L = mm_rcpf(fmaf(u, u, 1.0f));
-                    const float ru = tr.c1g * L;
-#pragma unroll
-                    for (int ee = 0; ee < NEMAX; ee++)
-                        if (ee == e) Rf[ee] += ru;
-                    f = fmaf(tr.hkf, ru, f);
-                    s = fmaf(tr.c2, L, s);
-                }
-            }
-            const float sat = mm_rcpf(1.0f + s);
-            double rs = 0.0;
-#pragma unroll
-            for (int e = 0; e < NEMAX; e++) {
-                R[c][e] = (double)(Rf[e] * sat);
-                rs += R[c][e];
-            }
-            Rk[c] = rs;
-            Fk[c] = (double)(f * sat);
         }
+        // saturation correction 1/(1 + s_total[g]) (rate_equations_jit.py:85-90)
+        const double sat = mm_rcp(1.0 + s);
+        satk[c] = sat;
+        double rs = 0.0;
+#pragma unroll
+        for (int e = 0; e < NEMAX; e++) {
+            R[c][e] = Rr[e] * sat;
+            rs += R[c][e];
+        }
+        Rk[c] = rs;
+        Fk[c] = f * sat;
     }
 
     // ---------------- columns of M' (FP64), replicated right-hand side ----------------
@@ -471,106 +409,6 @@ __device__ __forceinline__ PointOut solve_point(const ForceParams &P, const SetV
         }
     });
 
-    if (FP32) {
-        // ---------- one FP64 residual-refinement step: M' dx = e_last - M' x ----------
-        // M' x via the low-rank form M = BR^T R^T - diag(sum_e R): w_e = sum_k R[k,e] x_k.
-        double w[NEMAX];
-#pragma unroll
-        for (int e = 0; e < NEMAX; e++) {
-            double a = 0.0;
-#pragma unroll
-            for (int c = 0; c < CPL; c++) {
-                const int j = c * G + t;
-                if (EXACT ? (j < NGMAX) : (j < n_g)) a = fma(R[c][e], xs[c], a);
-            }
-            w[e] = mm_group_sum(a, G);
-        }
-        double sx = 0.0;
-#pragma unroll
-        for (int c = 0; c < CPL; c++) sx += xs[c];
-        sx = mm_group_sum(sx, G);
-        // residual of row g, evaluated by the lane owning column g
-        double rr[CPL];
-#pragma unroll
-        for (int c = 0; c < CPL; c++) {
-            const int g = c * G + t;
-            double r = 0.0;
-            if (EXACT ? (g < NGMAX) : (g < n_g)) {
-                if (g == n_g - 1) {
-                    r = 1.0 - sx;
-                } else {
-                    double mx = -Rk[c] * xs[c];
-#pragma unroll
-                    for (int e = 0; e < NEMAX; e++)
-                        if (EXACT || e < n_e) mx = fma(S.BR[e * n_g + g], w[e], mx);
-                    r = -mx;
-                }
-            }
-            rr[c] = r;
-        }
-        if (__any_sync(FULL, swapped)) {
-            // general permutation: gather the residual in every lane, apply the swaps
-            double rfull[NGMAX];
-            static_for<0, NGMAX>([&](auto gc) {
-                constexpr int g = decltype(gc)::value;
-                rfull[g] = __shfl_sync(FULL, rr[g / G], gbase + g % G);
-            });
-#pragma unroll
-            for (int col = 0; col < NGMAX; col++) {
-#pragma unroll
-                for (int r = col + 1; r < NGMAX; r++)
-                    if (r == prows[col]) { const double tmp = rfull[col]; rfull[col] = rfull[r]; rfull[r] = tmp; }
-            }
-            static_for<0, CPL>([&](auto cc) {
-                constexpr int c = decltype(cc)::value;
-#pragma unroll
-                for (int g = c * G; g < c * G + G && g < NGMAX; g++)
-                    if (g == c * G + t) rr[c] = rfull[g];
-            });
-        }
-        // forward substitution with the unit-lower L (factors stored below the diagonal)
-        static_for<0, NGMAX>([&](auto ic) {
-            constexpr int i = decltype(ic)::value;
-            constexpr int own = i % G, li = i / G;
-            if (EXACT || i < n_g) {
-                double part = 0.0;
-                static_for<0, CPL>([&](auto cc) {
-                    constexpr int c = decltype(cc)::value;
-                    if constexpr (c * G + G - 1 < i) {
-                        part = fma(A[c][i], rr[c], part);
-                    } else if constexpr (c * G < i) {
-                        if (c * G + t < i) part = fma(A[c][i], rr[c], part);
-                    }
-                });
-                part = mm_group_sum(part, G);
-                if (t == own) rr[li] -= part;
-            }
-        });
-        // backward substitution with U
-        double dx[CPL];
-#pragma unroll
-        for (int c = 0; c < CPL; c++) dx[c] = 0.0;
-        static_for<0, NGMAX>([&](auto iic) {
-            constexpr int i = NGMAX - 1 - decltype(iic)::value;
-            constexpr int own = i % G, li = i / G;
-            if (EXACT || i < n_g) {
-                double part = 0.0;
-                static_for<0, CPL>([&](auto cc) {
-                    constexpr int c = decltype(cc)::value;
-                    if constexpr (c * G > i) {
-                        part = fma(A[c][i], dx[c], part);
-                    } else if constexpr (c * G + G - 1 > i) {
-                        if (c * G + t > i) part = fma(A[c][i], dx[c], part);
-                    }
-                });
-                part = mm_group_sum(part, G);
-                if (t == own) dx[li] = (rr[li] - part) * invU[li];
-            }
-        });
-#pragma unroll
-        for (int c = 0; c < CPL; c++) xs[c] += dx[c];
-    }
-
     // ---------------- clamp, normalise, force ----------------
     double tot = 0.0;
 #pragma unroll
@@ -605,7 +443,7 @@ __device__ __forceinline__ PointOut solve_point(const ForceParams &P, const SetV
     out.F = mm_group_sum(F, G);
     out.R = mm_group_sum(Rs, G);
     out.gB = 0.0;
-    if constexpr (ADJ && !FP32) {
+    if constexpr (ADJ) {
         // ---------- adjoint: dF/dtheta = sum_{b,g,e} (p_g hk_b - mu[g,e]) d rate_bge / dtheta ----------
         // with lambda solving M'^T lambda = dF/dp = F_g and
         // mu[g,e] = p_g (sum_{g'<n-1} lambda_g' BR[e,g'] - lambda_g [g<n-1]) (implicit differentiation

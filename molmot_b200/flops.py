@@ -6,10 +6,9 @@ active (beam, ground, excited) triples (d2 >= 1e-15 for the beam's
 polarisation).  For SrOH with the 8-beam DC MOT, A = 96 and the total is
 about 4.82 kFLOP per point.
 
-The FP32-bulk form performs the per-triple rate work (18 A) and the
-per-state shift/doppler prelude in FP32 and everything from the population
-matrix on in FP64, plus the refinement step (residual 2 n_g^2 + triangular
-solves n_g^2).
+flops_per_point counts the plain form (the reference's algorithm);
+flops_reduced counts the FP32-bulk and FP64-reduced forms, which solve the
+populations through the excited-state chain.
 """
 from __future__ import annotations
 
@@ -22,9 +21,9 @@ def active_triples(d_squared, pols) -> int:
     return int(sum(int((d2[:, :, int(q)] >= 1e-15).sum()) for q in np.asarray(pols).ravel()))
 
 
-def flops_per_point(n_g: int, n_e: int, n_b: int, A: int, refine: bool = False):
-    """Returns (fp64_flops, fp32_flops) of one point.  With refine=False all
-    work is FP64 (the plain form)."""
+def flops_per_point(n_g: int, n_e: int, n_b: int, A: int):
+    """(fp64_flops, 0.0) of one point of the plain form (the reference's
+    algorithm, all FP64)."""
     n_s = n_g + n_e
     prelude = 3 * n_s + 3 * n_b
     rates = 18 * A
@@ -33,11 +32,7 @@ def flops_per_point(n_g: int, n_e: int, n_b: int, A: int, refine: bool = False):
     lu = sum(m * (2 * m + 5) for m in range(n_g))
     back = n_g * n_g
     tail = 2 * n_g + 4 * n_g * n_e
-    if not refine:
-        return float(prelude + rates + sat + build + lu + back + tail), 0.0
-    fp32 = prelude + rates + sat
-    fp64 = build + lu + back + tail + 3 * n_g * n_g
-    return float(fp64), float(fp32)
+    return float(prelude + rates + sat + build + lu + back + tail), 0.0
 
 
 def flops_reduced(n_g: int, n_e: int, A: int):
