@@ -115,6 +115,20 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def hbm_figure(nbytes, ms):
+    """Secondary HBM figure of the force kernel: algorithmic bytes per launch
+    over its time, against the measured copy bandwidth of MEASURED_PEAKS.json
+    (6.65 TB/s, an earlier measurement on this GPU type, if that file is absent)."""
+    peak, src = 6650.0, "fallback"
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peak, src = float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        pass
+    gbs = nbytes / (ms * 1e-3) / 1e9
+    return {"achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak, "peak_source": src}
+
+
 def peak_probe(torch):
     """Measured FP64 and FP32 FMA throughput (TFLOP/s) of this GPU."""
     import ctypes
@@ -473,6 +487,7 @@ def main():
                          "traffic": TRAFFIC_PER_LAUNCH if n_sets == N_SETS else None,
                          "traffic_unit": "bytes per launch",
                          "algorithmic_bytes": 8 * n_pts,
+                         "hbm": hbm_figure(8 * n_pts, ms32),
                          "peak_source": "mm_peak_probe FMA loop on this GPU: "
                                         f"fp64 {peaks['fp64']:.2f}, fp32 {peaks['fp32']:.2f} TFLOP/s",
                          "flops_per_point": {"fp64": f64_32, "fp32": f32_32},
