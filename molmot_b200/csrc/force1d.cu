@@ -1,11 +1,17 @@
 // force1d.cu -- batched 1D steady-state force and fused 1D trajectory
-// kernels, and their C-ABI entry points (mm_force_batch, mm_traj1d_run).
+// kernels, and their C-ABI entry points (mm_force_batch, mm_force_adjoint,
+// mm_traj_run, mm_traj1d_run).
 //
 // One CTA works on one parameter set: its prologue stages the molecule and
 // the set's beams into shared memory and compacts the active
-// (ground, beam, excited) triples; then groups of G lanes stream over the
-// set's points.  The trajectory kernel gives each group one particle and
-// runs the whole Euler loop in registers.
+// (ground, beam, excited) triples; then its threads stream over the set's
+// points.
+//  * Plain FP64 form (force_kernel, force_adjoint_kernel, traj1d_kernel):
+//    groups of G = 4 lanes per point, the reference's elimination
+//    (rate_core.cuh); the trajectory kernel runs a particle per group.
+//  * FP32-bulk and FP64-reduced forms (force_reduced_kernel,
+//    traj1d_reduced_kernel): one point or particle per thread, populations
+//    from the excited-state chain (reduced.cuh).
 #include <stdio.h>
 #include <algorithm>
 #include "rate_core.cuh"
