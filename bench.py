@@ -220,9 +220,16 @@ def secondary_measurements(torch, mol, pack, dev):
     tf = _ev_time(torch, lambda: force_batch(pack, bsa, v, z, points_per_set=66, want_pop=False,
                                              want_R=False, want_status=False), 5)
     ta = _ev_time(torch, lambda: force_adjoint(pack, bsa, v, z, points_per_set=66), 5)
+    trf = _ev_time(torch, lambda: force_batch(pack, bsa, v, z, points_per_set=66, want_pop=False,
+                                              want_R=False, want_status=False,
+                                              precision="fp64_reduced"), 5)
+    tra = _ev_time(torch, lambda: force_adjoint(pack, bsa, v, z, points_per_set=66,
+                                                precision="fp64_reduced"), 5)
     out["adjoint"] = {"workload": "1024 parameter sets x (33 z + 33 v) stencil points, gradients "
                                   "w.r.t. 8 beam frequencies, 8 s0 and B'",
-                      "forward_ms": tf, "forward_plus_adjoint_ms": ta, "cost_ratio": ta / tf}
+                      "forward_ms": tf, "forward_plus_adjoint_ms": ta, "cost_ratio": ta / tf,
+                      "reduced": {"forward_ms": trf, "forward_plus_adjoint_ms": tra,
+                                  "cost_ratio": tra / trf, "vs_elimination_adjoint": ta / tra}}
     out["uneven"] = uneven_measurement(torch, dev)
     return out
 

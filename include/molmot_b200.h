@@ -143,6 +143,10 @@ MM_API int mm_force_batch(const mm_pack *pack, const mm_beams *beams, const doub
  * _rate_eq_core.  grad: [n][2 n_beams + 1] rows
  * (dF/dfreq_b, b = 0..n_beams-1; dF/ds0_b; dF/dB'), Newton per Hz, per unit
  * s0 and per T/m.  Same layouts as mm_force_batch.
+ * opts->precision: MM_PREC_FP64 (the elimination adjoint) or
+ * MM_PREC_FP64_REDUCED (the adjoint of the excited-chain solve, one point per
+ * thread; when any set fails the reduced form's structural checks the whole
+ * batch runs the elimination adjoint).  Other precisions are rejected.
  */
 MM_API int mm_force_adjoint(const mm_pack *pack, const mm_beams *beams, const double *v,
                             const double *z, int64_t n_points, const mm_batch_opts *opts,

@@ -108,6 +108,7 @@ extern "C" int mm_pack_create(const mm_mol_desc *d, mm_pack **out)
         if (!isfinite(h[i])) { mm_set_error("molecule data contains a non-finite value"); delete p; return -1; }
     p->act.resize((size_t)n_g * n_e * 3);
     for (size_t i = 0; i < p->act.size(); i++) p->act[i] = d->d_squared[i] >= 1e-15 ? 1 : 0;
+    p->h_br.assign(h.begin() + p->oBR, h.begin() + p->oBR + (size_t)n_e * n_g);
     if (upload(&p->buf, h.data(), o)) { delete p; return -3; }
     *out = p;
     return 0;

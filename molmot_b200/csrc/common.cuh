@@ -35,6 +35,7 @@ struct mm_pack {
     // offsets (in doubles) into buf
     size_t oE, ozd, od2, oBR, oZre, oZim, oZe, oTdm;
     std::vector<unsigned char> act;  // host: d2[g][e][q] >= 1e-15 (active triple pattern)
+    std::vector<double> h_br;        // host: branching ratios BR[e][g]
 };
 
 // Device-resident parameter sets of beams.

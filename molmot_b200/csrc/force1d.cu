@@ -202,6 +202,71 @@ force_reduced_kernel(ForceParams P)
     }
 }
 
+// FP64-reduced adjoint: the FP64-reduced force and its gradient (same row
+// layout as force_adjoint_kernel), one point per thread.  The host launches it
+// only when every set passes the reduced form's structural checks.  Shared
+// scratch per thread: Doppler-shifted frequencies, dF/dfreq_b and dF/ds0_b
+// (3 n_b doubles, stride blockDim.x).
+template <int NGMAX, int NEMAX, bool EXACT, int PAD>
+__global__ void __launch_bounds__(kRedThreads, 2)
+force_reduced_adjoint_kernel(ForceParams P, double *grad)
+{
+    extern __shared__ __align__(16) unsigned char sm[];
+    RedLayout<NGMAX, NEMAX> Ly;
+    Ly.build(P.n_b);
+    const long long pts_per_set = (P.layout == MM_LAYOUT_GRID) ? P.nv * P.nz : P.pps;
+    const int nb = P.n_b, gw = 2 * nb + 1, st = blockDim.x;
+    double *fd = (double *)(sm + Ly.total) + threadIdx.x;
+    double *gf = fd + (size_t)nb * st, *gs = gf + (size_t)nb * st;
+    for (int set = blockIdx.y; set < P.n_sets; set += gridDim.y) {
+        const long long set_first = (long long)set * pts_per_set;
+        long long set_count = pts_per_set;
+        if (set_first + set_count > P.n_points) set_count = P.n_points - set_first;
+        if (set_count <= 0) continue;
+        RedView S;
+        __syncthreads();
+        build_reduced_tables<NGMAX, NEMAX, PAD, true>(P, set, sm, Ly, S);
+        const double Bg = P.bgrad[set];
+        const int32_t *pol = P.pol + (size_t)set * nb;
+        const long long chunk = (set_count + gridDim.x - 1) / gridDim.x;
+        const long long start = (long long)blockIdx.x * chunk;
+        const long long end = min(start + chunk, set_count);
+        for (long long ip = start + threadIdx.x; ip < end; ip += st) {
+            double v, z;
+            if (P.layout == MM_LAYOUT_GRID) {
+                v = P.v[ip / P.nz];
+                z = P.z[ip % P.nz];
+            } else {
+                v = P.v[set_first + ip];
+                z = P.z[set_first + ip];
+            }
+            const long long gi = set_first + ip;
+            double *row = grad + gi * gw;
+            if (!(isfinite(v) && isfinite(z))) {
+                const double nan = __longlong_as_double(0x7ff8000000000000ll);
+                P.F[gi] = nan;
+                if (P.status) P.status[gi] = MM_ST_NONFINITE;
+                for (int i = 0; i < gw; i++) row[i] = nan;
+                continue;
+            }
+            for (int b = 0; b < nb; b++) {
+                gf[b * st] = 0.0;
+                gs[b * st] = 0.0;
+            }
+            double gB;
+            const RedOut o = reduced_adjoint_point<NGMAX, NEMAX, EXACT, PAD>(P, S, pol, v, z, Bg, fd, st,
+                                                                             gf, gs, gB);
+            P.F[gi] = o.F;
+            if (P.status) P.status[gi] = o.status;
+            for (int b = 0; b < nb; b++) {
+                row[b] = gf[b * st];
+                row[nb + b] = gs[b * st];
+            }
+            row[2 * nb] = gB;
+        }
+    }
+}
+
 struct TrajParams {
     double dt, z_escape, mass;
     long long n_particles, n_steps;
@@ -499,6 +564,32 @@ int launch_adjoint(const ForceParams &P, double *grad, cudaStream_t st)
     return mm_cuda_check(cudaGetLastError(), "force_adjoint_kernel launch") ? -3 : 0;
 }
 
+template <class C, int PAD>
+int launch_reduced_adjoint(const ForceParams &P, double *grad, cudaStream_t st)
+{
+    auto kern = force_reduced_adjoint_kernel<C::ng, C::ne, C::exact, PAD>;
+    RedLayout<C::ng, C::ne> Ly;
+    Ly.build(P.n_b);
+    const size_t sb = Ly.total + sizeof(double) * 3 * P.n_b * kRedThreads;
+    if (sb > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb);
+        if (mm_cuda_check(e, "cudaFuncSetAttribute")) return -3;
+    }
+    int dev = 0, nsm = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kRedThreads, sb);
+    if (per_sm < 1) per_sm = 1;
+    const long long pts_per_set = (P.layout == MM_LAYOUT_GRID) ? P.nv * P.nz : P.pps;
+    const long long want = (long long)nsm * per_sm * 4;
+    long long gx = std::max<long long>(1, want / std::max(1, P.n_sets));
+    gx = std::min(gx, std::max<long long>(1, (pts_per_set + kRedThreads * 4 - 1) / (kRedThreads * 4)));
+    gx = std::min<long long>(gx, 1 << 20);
+    dim3 grid((unsigned)gx, (unsigned)std::min(P.n_sets, 65535));
+    kern<<<grid, kRedThreads, sb, st>>>(P, grad);
+    return mm_cuda_check(cudaGetLastError(), "force_reduced_adjoint_kernel launch") ? -3 : 0;
+}
+
 template <class C>
 int launch_traj(const ForceParams &P, const TrajParams &T, cudaStream_t st)
 {
@@ -534,6 +625,46 @@ int reduced_list_granule(const mm_pack *pack, const mm_beams *beams)
         }
     }
     return (4 * n_pad <= 5 * n_raw) ? kRedPad : 1;
+}
+
+// True when every set of the batch passes the reduced form's structural
+// checks (the host twin of build_reduced_tables' flags[0]): every ground state
+// has a triple, and the excited chain e' -> e (e' decays to a ground state
+// that a beam of the set excites to e) is strongly connected.
+bool reduced_all_valid(const mm_pack *pack, const mm_beams *beams)
+{
+    const int n_g = pack->n_g, n_e = pack->n_e, n_b = beams->n_b;
+    if (n_e > 32) return false;
+    std::vector<int> cnt((size_t)n_g * n_e);
+    for (int s = 0; s < beams->n_sets; s++) {
+        int npol[3] = {0, 0, 0};
+        for (int b = 0; b < n_b; b++) npol[beams->h_pol[(size_t)s * n_b + b]]++;
+        for (int i = 0; i < n_g * n_e; i++) {
+            const unsigned char *a = &pack->act[(size_t)i * 3];
+            cnt[i] = a[0] * npol[0] + a[1] * npol[1] + a[2] * npol[2];
+        }
+        for (int g = 0; g < n_g; g++) {
+            int c = 0;
+            for (int e = 0; e < n_e; e++) c += cnt[g * n_e + e];
+            if (c == 0) return false;
+        }
+        unsigned T[32];
+        for (int i = 0; i < n_e; i++) {
+            unsigned ti = 1u << i;
+            for (int g = 0; g < n_g; g++)
+                if (pack->h_br[(size_t)i * n_g + g] > 0.0)
+                    for (int j = 0; j < n_e; j++)
+                        if (cnt[g * n_e + j] > 0) ti |= 1u << j;
+            T[i] = ti;
+        }
+        for (int k = 0; k < n_e; k++)
+            for (int i = 0; i < n_e; i++)
+                if (T[i] >> k & 1u) T[i] |= T[k];
+        const unsigned all = (n_e == 32) ? ~0u : (1u << n_e) - 1u;
+        for (int i = 0; i < n_e; i++)
+            if ((T[i] & all) != all) return false;
+    }
+    return true;
 }
 
 // Size-class dispatch.  SrOH (12 ground, 4 excited) has an exact class.
@@ -582,10 +713,21 @@ extern "C" int mm_force_adjoint(const mm_pack *pack, const mm_beams *beams, cons
     const int rc = prepare_batch(pack, beams, v, z, n_points, opts, F, P, pps);
     if (rc <= 0) return rc;
     if (!grad) { mm_set_error("grad must be non-null"); return -1; }
-    if (opts->precision != MM_PREC_FP64) { mm_set_error("the adjoint runs in the FP64 form only"); return -1; }
+    if (opts->precision != MM_PREC_FP64 && opts->precision != MM_PREC_FP64_REDUCED) {
+        mm_set_error("the adjoint runs in the FP64 and FP64-reduced forms only");
+        return -1;
+    }
     P.R = nullptr; P.pop = nullptr; P.status = nullptr;
     cudaStream_t st = (cudaStream_t)stream;
-    return dispatch_class(P.n_g, P.n_e, [&](auto C) -> int { return launch_adjoint<decltype(C)>(P, grad, st); });
+    // FP64-reduced: the reduced adjoint when every set is structurally valid,
+    // else the elimination adjoint for the whole batch
+    const bool red = opts->precision == MM_PREC_FP64_REDUCED && reduced_all_valid(pack, beams);
+    return dispatch_class(P.n_g, P.n_e, [&](auto C) -> int {
+        using CT = decltype(C);
+        if (!red) return launch_adjoint<CT>(P, grad, st);
+        return reduced_list_granule(pack, beams) == kRedPad ? launch_reduced_adjoint<CT, kRedPad>(P, grad, st)
+                                                             : launch_reduced_adjoint<CT, 1>(P, grad, st);
+    });
 }
 
 // Validates a batch call and fills P; returns 1 to launch, 0 for an empty

@@ -210,6 +210,7 @@ __device__ void build_reduced_tables(const ForceParams &P, int set, unsigned cha
         for (; o < offs[i + 1]; o++) {  // zero-weight padding: every term 0
             if constexpr (F64) {
                 TripD tr = {};
+                tr.pad = 1;  // marks list padding for the adjoint
                 tripd[o] = tr;
             } else {
                 TripR tr = {};
@@ -494,5 +495,173 @@ __device__ __forceinline__ RedOut reduced_point(const ForceParams &P, const RedV
         }
     }
     if (!ok || !isfinite(o.F)) o.status |= MM_ST_NONFINITE;
+    return o;
+}
+
+// ---------------------------------------------------------------------------
+// Adjoint of the FP64-reduced form: F and dF/d(freq_b, s0_b, B') at one point
+// (one thread).  With u = dF/dpi = (cf - F cw) / norm (u . pi = 0) and lambda
+// solving (I - K)^T lambda = u (lambda_0 = 0: K's columns sum to one, so
+// lambda is defined up to a multiple of the ones vector, which dK annihilates),
+//     dF = sum_g [ y_g sum_e lambda_e d a_ge + (y_g / norm) d phi_g
+//                  - (F y_g / norm) d w_g ],   y_g = sum_e BR[e,g] pi_e,
+// and a_ge, phi_g, w_g are functions of the unsaturated rate sums R_ge, the
+// force sum f_g and the saturation sum s_g.  Each triple (g, b, e) enters
+// those sums through c1 L, hk c1 L and c2 L, so its contribution is
+//     q = alpha_ge c1 + beta_g hk c1 + gamma_g c2   times dL,
+// with dL/dfreq_b = L'(delta) 2 pi, dL/dB' = L'(delta) (-z 1e4 (zd_e - zd_g)
+// Gamma) and d(c1, c2)/ds0_b = (c1, c2) / s0_b written with d2 (s0_b may be 0).
+// gf[b * stride], gs[b * stride]: this thread's per-beam accumulators
+// (shared memory); the caller zeroes them.  pol: the set's polarisations.
+// Valid sets only (S.valid); finite v and z.
+template <int NGMAX, int NEMAX, bool EXACT, int PAD>
+__device__ __forceinline__ RedOut reduced_adjoint_point(const ForceParams &P, const RedView &S,
+                                                        const int32_t *pol, double v, double z,
+                                                        double Bgrad, double *fd, int stride,
+                                                        double *gf, double *gs, double &gB)
+{
+    const int n_g = EXACT ? NGMAX : P.n_g;
+    const int n_e = EXACT ? NEMAX : P.n_e;
+    RateCtx<NEMAX> C;
+    C.B = __dmul_rn(__dmul_rn(Bgrad, z), 1e4);
+    C.fd = fd;
+    C.stride = stride;
+    for (int b = 0; b < P.n_b; b++)
+        fd[b * stride] = __dadd_rn(S.freq[b], __ddiv_rn(__dmul_rn(S.ck[b], v), MM_TWO_PI));
+#pragma unroll
+    for (int e = 0; e < NEMAX; e++)
+        C.Ese[e] = (e < n_e) ? __dadd_rn(S.E[n_g + e], __ddiv_rn(__dmul_rn(__dmul_rn(C.B, S.zde[e]), P.Gamma),
+                                                                  MM_TWO_PI))
+                             : 0.0;
+    const double gh = P.Gamma / 2.0, gh2 = gh * gh;
+
+    // forward: K, cw, cf and the stationary vector
+    double K[NEMAX][NEMAX], K0[NEMAX][NEMAX], cw[NEMAX], cf[NEMAX];
+#pragma unroll
+    for (int e = 0; e < NEMAX; e++) {
+        cw[e] = 0.0;
+        cf[e] = 0.0;
+#pragma unroll
+        for (int e2 = 0; e2 < NEMAX; e2++) K[e][e2] = 0.0;
+    }
+    for (int g = 0; g < n_g; g++) {
+        double Re[NEMAX], f, s;
+        reduced_rates<NEMAX, PAD, true>(S, g, C, gh2, Re, f, s);
+        double rt = 0.0;
+#pragma unroll
+        for (int e = 0; e < NEMAX; e++) rt += Re[e];
+        const double inv = mm_rcp(rt);
+        const double phi = f * inv, w = (1.0 + s) * inv;
+#pragma unroll
+        for (int e = 0; e < NEMAX; e++) {
+            const double br = S.brt[g * NEMAX + e];
+            cw[e] = fma(br, w, cw[e]);
+            cf[e] = fma(br, phi, cf[e]);
+#pragma unroll
+            for (int e2 = 0; e2 < NEMAX; e2++) K[e2][e] = fma(Re[e2] * inv, br, K[e2][e]);
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < NEMAX; i++)
+#pragma unroll
+        for (int j = 0; j < NEMAX; j++) K0[i][j] = K[i][j];
+    double pi[NEMAX];
+    const bool ok = gth_stationary<NEMAX>(K, n_e, pi);
+    double nrm = 0.0, fn = 0.0, rn = 0.0;
+#pragma unroll
+    for (int e = 0; e < NEMAX; e++) {
+        nrm = fma(cw[e], pi[e], nrm);
+        fn = fma(cf[e], pi[e], fn);
+        rn = fma(S.rsum[e], pi[e], rn);
+    }
+    const double in = mm_rcp(nrm);
+    const double F = fn * in;
+
+    // adjoint of the chain: lambda_0 = 0, (delta_kj - K0[j][k]) lambda_j = u_k for k, j >= 1
+    double lam[NEMAX], A[NEMAX][NEMAX];
+#pragma unroll
+    for (int k = 0; k < NEMAX; k++) {
+        lam[k] = (k >= 1 && k < n_e) ? (cf[k] - F * cw[k]) * in : 0.0;
+#pragma unroll
+        for (int j = 0; j < NEMAX; j++) A[k][j] = ((k == j) ? 1.0 : 0.0) - ((k < n_e && j < n_e) ? K0[j][k] : 0.0);
+    }
+    // elimination without pivoting on rows/columns 1..n_e-1 (an M-matrix for a
+    // strongly connected chain), then back substitution
+#pragma unroll
+    for (int c = 1; c < NEMAX; c++) {
+        if (c < n_e) {
+            const double ip = mm_rcp(A[c][c]);
+#pragma unroll
+            for (int r = c + 1; r < NEMAX; r++) {
+                if (r < n_e) {
+                    const double m = A[r][c] * ip;
+#pragma unroll
+                    for (int j = c + 1; j < NEMAX; j++) A[r][j] = fma(-m, A[c][j], A[r][j]);
+                    lam[r] = fma(-m, lam[c], lam[r]);
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int c = NEMAX - 1; c >= 1; c--) {
+        if (c < n_e) {
+            double a = lam[c];
+#pragma unroll
+            for (int j = c + 1; j < NEMAX; j++)
+                if (j < n_e) a = fma(-A[c][j], lam[j], a);
+            lam[c] = a * mm_rcp(A[c][c]);
+        }
+    }
+    lam[0] = 0.0;
+
+    // second pass: per ground state coefficients, then the triples once more
+    gB = 0.0;
+    const double inrm = in, Fin = F * in;
+    for (int g = 0; g < n_g; g++) {
+        double Re[NEMAX], f, s;
+        reduced_rates<NEMAX, PAD, true>(S, g, C, gh2, Re, f, s);
+        double rt = 0.0, yg = 0.0;
+#pragma unroll
+        for (int e = 0; e < NEMAX; e++) {
+            rt += Re[e];
+            yg = fma(S.brt[g * NEMAX + e], pi[e], yg);
+        }
+        const double inv = mm_rcp(rt);
+        const double phi = f * inv, w = (1.0 + s) * inv;
+        double Lam = 0.0;
+#pragma unroll
+        for (int e = 0; e < NEMAX; e++) Lam = fma(lam[e], Re[e] * inv, Lam);
+        const double yi = yg * inv;
+        const double beta = yi * inrm, gamma = -yi * Fin;
+        const double common = -Lam - phi * inrm + w * Fin;
+        const double Esg = fma(C.B, S.czd[g], S.E[g]);
+#pragma unroll
+        for (int e = 0; e < NEMAX; e++) {
+            const double alpha = yi * (lam[e] + common);
+            const int i0 = S.offs[g * NEMAX + e], i1 = S.offs[g * NEMAX + e + 1];
+            const double om = __dsub_rn(C.Ese[e], Esg);
+            const double dBde = -z * 1e4 * (S.zde[e] - P.zd[g]) * P.Gamma;  // d delta / dB'
+            for (int i = i0; i < i1; i++) {
+                const TripD tr = ((const TripD *)S.trip)[i];
+                if (tr.pad) continue;  // list padding
+                const int b = tr.b;
+                const double de = __dmul_rn(__dsub_rn(fd[b * stride], om), MM_TWO_PI);
+                const double iden = mm_rcp(fma(de, de, gh2));
+                const double L = gh2 * iden;
+                const double dLd = -2.0 * de * L * iden;  // dL / d delta
+                const double q = fma(alpha + beta * tr.hk, tr.c1, gamma * tr.c2);
+                gf[b * stride] = fma(q * dLd, MM_TWO_PI, gf[b * stride]);
+                // d(c1, c2)/ds0_b with d2 = c2 / s0_b written out: c1 = ((Gamma/2) s0 d2) Geff
+                const double d2 = P.d2[(g * P.n_e + e) * 3 + pol[b]];
+                const double qs = fma((alpha + beta * tr.hk) * gh * P.geff, d2, gamma * d2);
+                gs[b * stride] = fma(qs, L, gs[b * stride]);
+                gB = fma(q * dLd, dBde, gB);
+            }
+        }
+    }
+    RedOut o;
+    o.F = F;
+    o.R = rn * in;
+    o.status = (!ok || !isfinite(F)) ? MM_ST_NONFINITE : 0;
     return o;
 }

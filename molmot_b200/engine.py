@@ -413,19 +413,25 @@ def traj3d(pack: MoleculePack, beams: BeamSets, r0, v0, dt: float, n_steps: int,
 
 
 def force_adjoint(pack: MoleculePack, beams: BeamSets, v, z, *, grid: bool = False,
-                  points_per_set: Optional[int] = None, hbar=None, stream=None):
-    """Force and its gradient (FP64): returns (F [n], grad [n, 2 n_beams + 1]) device
-    tensors; grad rows are (dF/dfreq_b..., dF/ds0_b..., dF/dB')."""
+                  points_per_set: Optional[int] = None, hbar=None, precision: str = "fp64",
+                  stream=None):
+    """Force and its gradient: returns (F [n], grad [n, 2 n_beams + 1]) device
+    tensors; grad rows are (dF/dfreq_b..., dF/ds0_b..., dF/dB').  precision:
+    "fp64" (the elimination adjoint) or "fp64_reduced" (the adjoint of the
+    excited-chain solve; batches with a set that fails its structural checks
+    run the elimination adjoint)."""
+    if precision not in ("fp64", "fp64_reduced"):
+        raise ValueError(f"the adjoint runs in the fp64 and fp64_reduced forms, not {precision!r}")
     v = _to_dev(v)
     z = _to_dev(z)
     nb = beams.n_beams
     if grid:
         nv, nz = v.numel(), z.numel()
         n = beams.n_sets * nv * nz
-        opts = _opts("fp64", _lib.MM_LAYOUT_GRID, nv=nv, nz=nz, hbar=hbar)
+        opts = _opts(precision, _lib.MM_LAYOUT_GRID, nv=nv, nz=nz, hbar=hbar)
     else:
         n = v.numel()
-        opts = _opts("fp64", _lib.MM_LAYOUT_POINTS, pps=points_per_set or n, hbar=hbar)
+        opts = _opts(precision, _lib.MM_LAYOUT_POINTS, pps=points_per_set or n, hbar=hbar)
     F = torch.empty(n, dtype=torch.float64, device=v.device)
     G = torch.empty((n, 2 * nb + 1), dtype=torch.float64, device=v.device)
     rc = _lib.load().mm_force_adjoint(pack.handle, beams.handle, _dptr(v), _dptr(z), n,

@@ -2,11 +2,16 @@
 MOT coefficients k, beta (33-point stencils) with respect to the 4
 detunings, 4 powers (s0) and B'.
 
-Checks:
+Both adjoint forms (precision "fp64": the elimination's transposed solve;
+"fp64_reduced": the excited-chain solve's transposed system) are checked:
   * against FP64 torch autograd of a dense restatement (oracle/torch_dense.py)
     -- tolerance 1e-8 of the largest gradient component per parameter set;
   * against central finite differences of the GPU forward with
-    h = 1e-4 relative (1e-3 for B') -- tolerance 1e-5 relative.
+    h = 1e-4 relative (1e-3 for B') -- tolerance 1e-5 relative;
+  * against each other on smaller molecules (1e-9 of the largest component);
+  * the reduced form's forward equals mm_force_batch's FP64-reduced force bit
+    for bit, and a batch with a structurally invalid set runs the elimination
+    adjoint (bit-identical to precision "fp64").
 """
 import numpy as np
 import pytest
@@ -41,7 +46,8 @@ def _params(ref, det, s0, B, dev):
     return f, p, b, freq, s0b
 
 
-def test_adjoint_vs_torch_autograd(mol, gpu):
+@pytest.mark.parametrize("precision", ["fp64", "fp64_reduced"])
+def test_adjoint_vs_torch_autograd(mol, gpu, precision):
     from molmot_b200.autograd import steady_state_force
     from oracle import torch_dense as td
     ref, det, s0, B, kdir, pol = _sets(mol, 6, 1)
@@ -51,7 +57,7 @@ def test_adjoint_vs_torch_autograd(mol, gpu):
     z = rng.uniform(-1e-2, 1e-2, 6 * pps)
     w = torch.as_tensor(rng.normal(size=6 * pps), dtype=torch.float64)
     f1, p1, b1, freq1, s01 = _params(ref, det, s0, B, gpu)
-    F1 = steady_state_force(mol, kdir, pol, freq1, s01, b1, v, z, pps)
+    F1 = steady_state_force(mol, kdir, pol, freq1, s01, b1, v, z, pps, precision=precision)
     (F1.cpu() * w).sum().backward()
     f2, p2, b2, freq2, s02 = _params(ref, det, s0, B, "cpu")
     F2 = td.force(mol, kdir, pol, freq2, s02, b2, v, z, pps)
@@ -63,11 +69,12 @@ def test_adjoint_vs_torch_autograd(mol, gpu):
         assert np.all(np.abs(ga - gb) <= 1e-8 * scale + 1e-300), (ga, gb)
 
 
-def test_mot_coefficient_gradients_vs_central_fd(mol, gpu):
+@pytest.mark.parametrize("precision", ["fp64", "fp64_reduced"])
+def test_mot_coefficient_gradients_vs_central_fd(mol, gpu, precision):
     from molmot_b200.autograd import mot_coefficients
     ref, det, s0, B, kdir, pol = _sets(mol, 4, 3)
     f, p, b, freq, s0b = _params(ref, det, s0, B, gpu)
-    k, beta = mot_coefficients(mol, kdir, pol, freq, s0b, b)
+    k, beta = mot_coefficients(mol, kdir, pol, freq, s0b, b, precision=precision)
     gk = torch.autograd.grad(k.sum(), [f, p, b], retain_graph=True)
     gbeta = torch.autograd.grad(beta.sum(), [f, p, b])
 
@@ -75,7 +82,7 @@ def test_mot_coefficient_gradients_vs_central_fd(mol, gpu):
         with torch.no_grad():
             _, _, _, fr, s0bb = _params(ref, det_, s0_, B_, gpu)
             bb = torch.tensor(B_, dtype=torch.float64, device=gpu)
-            kk, be = mot_coefficients(mol, kdir, pol, fr, s0bb, bb)
+            kk, be = mot_coefficients(mol, kdir, pol, fr, s0bb, bb, precision=precision)
         return kk.cpu().numpy(), be.cpu().numpy()
 
     for which, base in [(0, det), (1, s0), (2, B)]:
@@ -118,3 +125,59 @@ def test_adjoint_forward_equals_force_batch(mol, gpu):
     F2 = force_batch(pack_for(mol), bs, g["v"], g["z"], points_per_set=npts)["F"]
     assert torch.equal(F, F2)
     assert G.shape == (ns * npts, 17)
+
+
+def test_reduced_adjoint_forward_equals_reduced_force(mol, gpu):
+    import bench
+    from molmot_b200.engine import BeamSets, force_batch, force_adjoint, pack_for
+    bs = BeamSets(*bench.make_params(mol, 16, 7))
+    v = np.linspace(-10, 10, 24)
+    z = np.linspace(-1e-2, 1e-2, 20)
+    F, G = force_adjoint(pack_for(mol), bs, v, z, grid=True, precision="fp64_reduced")
+    F2 = force_batch(pack_for(mol), bs, v, z, grid=True, precision="fp64_reduced")["F"]
+    assert torch.equal(F, F2.reshape(-1))
+    Fp, Gp = force_adjoint(pack_for(mol), bs, v, z, grid=True, precision="fp64")
+    scale = Gp.view(16, -1, 17).abs().amax(dim=1, keepdim=True)
+    err = ((G - Gp).view(16, -1, 17).abs() / scale).nan_to_num(0.0)
+    assert float(err.max()) < 1e-9
+
+
+@pytest.mark.parametrize("n_g,n_e", [(4, 2), (7, 3), (9, 4)])
+def test_reduced_adjoint_smaller_molecules(gpu, n_g, n_e):
+    from molmot_b200.engine import BeamSets, MoleculePack, force_adjoint
+    from molmot_b200.molecules.synthetic import dc_beams_for, synthetic_molecule
+    m = synthetic_molecule(n_g, n_e, 100 + n_g)
+    kd, fr, po, s0 = dc_beams_for(m)
+    pk = MoleculePack(m)
+    bs = BeamSets(kd[None], fr[None], po[None], s0[None], [0.2])
+    v = np.linspace(-10, 10, 33)
+    z = np.linspace(-1e-2, 1e-2, 29)
+    Fr, Gr = force_adjoint(pk, bs, v, z, grid=True, precision="fp64_reduced")
+    Fp, Gp = force_adjoint(pk, bs, v, z, grid=True, precision="fp64")
+    assert float((Fr - Fp).abs().max()) <= 1e-12 * float(Fp.abs().max())
+    scale = Gp.abs().amax(dim=0)
+    assert float(((Gr - Gp).abs() / scale).nan_to_num(0.0).max()) < 1e-9
+
+
+def test_reduced_adjoint_invalid_set_runs_elimination(mol, gpu):
+    """A set whose beams are all pi leaves ground state 11 unpumped: the
+    batch runs the elimination adjoint, bit for bit."""
+    import bench
+    from molmot_b200.engine import BeamSets, force_adjoint, pack_for
+    kdir, freq, pol, s0, B = bench.make_params(mol, 3, 11)
+    pol = pol.copy()
+    pol[1] = 1
+    bs = BeamSets(kdir, freq, pol, s0, B)
+    v = np.linspace(-5, 5, 9)
+    z = np.linspace(-5e-3, 5e-3, 7)
+    Fr, Gr = force_adjoint(pack_for(mol), bs, v, z, grid=True, precision="fp64_reduced")
+    Fp, Gp = force_adjoint(pack_for(mol), bs, v, z, grid=True, precision="fp64")
+    assert torch.equal(Fr, Fp) and torch.equal(Gr.nan_to_num(7.0), Gp.nan_to_num(7.0))
+
+
+def test_adjoint_rejects_fp32(mol, gpu):
+    from molmot_b200.engine import BeamSets, force_adjoint, pack_for
+    g = golden("random_points.npz")
+    bs = BeamSets(g["kdir"][:1], g["freq"][:1], g["pol"][:1], g["s0"][:1], g["B"][:1])
+    with pytest.raises(ValueError):
+        force_adjoint(pack_for(mol), bs, g["v"][:4], g["z"][:4], precision="fp32")
