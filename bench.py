@@ -210,6 +210,27 @@ def secondary_measurements(torch, mol, pack, dev):
                           "particles": 65536, "steps": S1, "ms": ms,
                           "workload": "the same ensemble, FP32-bulk force (reduced solve), one "
                                       "particle per thread"}
+    # trajectory gradient: d<E_kin>/d(4 detunings) of the per-axis 3D model,
+    # 4096 particles x 1000 steps, kicks at fixed noise, checkpoints every 50 steps
+    from molmot_b200.trajgrad import traj_grad
+    NG, SG = 4096, 1000
+    rg = torch.as_tensor(rng.normal(0, 1e-3, (NG, 3)), device=dev)
+    vg = torch.as_tensor(rng.normal(0, sig_v, (NG, 3)), device=dev)
+    fpar = [0, 0, 1, 1, 2, 2, 3, 3]
+    run = lambda: traj_grad(pack, bs1, rg, vg, 1e-6, SG, n_par=4, freq_par=fpar, kicks=True,
+                            seed=SEED, ckpt_every=50)
+    msg = _ev_time(torch, run, 2)
+    msf = _ev_time(torch, lambda: traj(pack, bs1, rg, vg, 1e-6, SG + 1, ndim=3), 2)
+    g = run()
+    grad = (mol.mass * (g["v"][:, :, None] * g["dv"]).sum(1).mean(0)).cpu().numpy()
+    out["traj_grad"] = {"metric": "particle-steps/s", "value": NG * SG / (msg * 1e-3),
+                        "particles": NG, "steps": SG, "ms": msg, "forward_fp64_ms": msf,
+                        "cost_ratio_vs_fp64_forward": msg / msf,
+                        "dE_ddetuning_J_per_Hz": [float(x) for x in grad],
+                        "workload": "SrOH per-axis 3D quadrupole MOT (trajectories.py:78-156), DC "
+                                    "4-frequency beams, r ~ N(0, 1 mm), v ~ MB(5 mK), Euler dt=1us, "
+                                    "recoil kicks at fixed noise, tangents for the 4 detunings, "
+                                    "state checkpointed every 50 steps"}
     # adjoint: 1024 parameter sets x 66 stencil points (33 z + 33 v)
     kdir, freq, pol, s0, B = make_params(mol, 1024, SEED + 7)
     bsa = BeamSets(kdir, freq, pol, s0, B)

@@ -41,9 +41,10 @@ extern "C" {
 #define MM_PREC_FP32_REFINE 1  /* FP32-bulk: FP32 Lorentzians with FP64 sums, populations in FP64
                                   through the excited-state chain (reduced.cuh), one point or
                                   particle per thread (the name is kept for the ABI) */
-#define MM_PREC_FP64_REDUCED 2 /* mm_force_batch only: FP64 rates in the plain form's operation order,
-                                  populations from the same FP64 excited-chain solve as
-                                  MM_PREC_FP32_REFINE (agrees with MM_PREC_FP64 to rounding) */
+#define MM_PREC_FP64_REDUCED 2 /* mm_force_batch and mm_force_adjoint: FP64 rates in the plain
+                                  form's operation order, populations from the same FP64
+                                  excited-chain solve as MM_PREC_FP32_REFINE (agrees with
+                                  MM_PREC_FP64 to rounding) */
 
 /* point layouts of mm_force_batch */
 #define MM_LAYOUT_POINTS 0 /* v[i], z[i]; point i belongs to set i / points_per_set */
@@ -235,6 +236,43 @@ MM_API int mm_traj_run(const mm_pack *pack, const mm_beams *beams, const mm_traj
                        const double *r0, const double *v0, int64_t n_particles,
                        double *r_final, double *v_final, int32_t *n_actual, double *r_traj,
                        double *v_traj, double *vsq_sum, double *n_samp, void *stream);
+
+/* Options of mm_traj_grad_run. */
+#define MM_TGRAD_MAX_PAR 8
+typedef struct {
+    int64_t n_steps;     /* Euler steps in this call                                          */
+    int64_t step0;       /* absolute step index of the state passed in (0 for a new run)      */
+    int64_t ckpt_every;  /* with ckpt non-NULL: save the state after every ckpt_every-th step  */
+    double dt;           /* s                                                                 */
+    double r_escape;     /* m: |r| beyond which a particle stops                              */
+    double hbar;         /* J s; <= 0 selects 1.0545718e-34                                   */
+    uint64_t seed;       /* Philox key of the recoil kicks                                    */
+    int32_t kicks;       /* != 0: photon-recoil kicks, held fixed under differentiation       */
+    int32_t n_par;       /* parameters theta_k, 1..MM_TGRAD_MAX_PAR                           */
+    int32_t freq_par[MM_MAX_BEAMS]; /* parameter whose value adds to beam b's frequency, or -1 */
+    int32_t s0_par[MM_MAX_BEAMS];   /* parameter whose value adds to beam b's s0, or -1        */
+    int32_t bprime_par;  /* parameter that adds to B', or -1                                  */
+    int32_t reserved;
+} mm_tgrad_opts;
+
+/*
+ * Trajectories of the per-axis 3D MOT model (molmot/propagation/
+ * trajectories.py:78-156; the model of mm_traj_run with ndim = 3, beam set 0)
+ * carried with their tangents d(r, v)/d theta_k (forward mode, the force's
+ * gradient from the FP64-reduced adjoint each step).  Optional photon-recoil
+ * kicks as in mm_traj3d_run, with N ~ Poisson((R_x + R_y + R_z) dt) events per
+ * step.  No counterpart in the reference (new on this path).
+ * state [N][6 + 6 n_par] (device, in/out): r[3], v[3], dr[3][n_par], dv[3][n_par];
+ * n_actual [N] (device, in/out; 0 for a new run): the absolute step a particle
+ * stopped at, or step0 + n_steps.  ckpt [n_steps / ckpt_every][N][6 + 6 n_par]
+ * (nullable): the state after steps ckpt_every, 2 ckpt_every, ... of the call;
+ * passing checkpoint c back as state with step0 + (c + 1) ckpt_every resumes
+ * the run bit for bit.  Beam set 0 must pass the reduced form's structural
+ * checks (every ground state pumped, excited chain strongly connected).
+ */
+MM_API int mm_traj_grad_run(const mm_pack *pack, const mm_beams *beams, const mm_tgrad_opts *opts,
+                            int64_t n_particles, double *state, int32_t *n_actual, double *ckpt,
+                            void *stream);
 
 /*
  * N independent 1D trajectories with symplectic Euler, one beam set (set 0).

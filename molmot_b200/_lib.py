@@ -57,6 +57,18 @@ class TrajOpts(ctypes.Structure):
                 ("hbar", ctypes.c_double)]
 
 
+MM_TGRAD_MAX_PAR = 8
+
+
+class TgradOpts(ctypes.Structure):
+    _fields_ = [("n_steps", ctypes.c_int64), ("step0", ctypes.c_int64),
+                ("ckpt_every", ctypes.c_int64), ("dt", ctypes.c_double),
+                ("r_escape", ctypes.c_double), ("hbar", ctypes.c_double),
+                ("seed", ctypes.c_uint64), ("kicks", ctypes.c_int32), ("n_par", ctypes.c_int32),
+                ("freq_par", ctypes.c_int32 * MM_MAX_BEAMS), ("s0_par", ctypes.c_int32 * MM_MAX_BEAMS),
+                ("bprime_par", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+
+
 class UnevenOpts(ctypes.Structure):
     _fields_ = [("warps_per_cta", ctypes.c_int32 * 3), ("chunk_groups", ctypes.c_int32)]
 
@@ -100,6 +112,8 @@ SIGNATURES = {
     "mm_histogram": (ctypes.c_int, [_vp, ctypes.c_int64, ctypes.c_int64, ctypes.c_double, ctypes.c_double,
                                     ctypes.c_int32, _vp, _vp]),
     "mm_peak_probe": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int64, _dp, _dp, _vp]),
+    "mm_traj_grad_run": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(TgradOpts), ctypes.c_int64, _vp, _vp,
+                                        _vp, _vp]),
 }
 
 _lib = None

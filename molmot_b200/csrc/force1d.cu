@@ -1,6 +1,6 @@
 // force1d.cu -- batched 1D steady-state force and fused 1D trajectory
 // kernels, and their C-ABI entry points (mm_force_batch, mm_force_adjoint,
-// mm_traj_run, mm_traj1d_run).
+// mm_traj_run, mm_traj1d_run, mm_traj_grad_run).
 //
 // One CTA works on one parameter set: its prologue stages the molecule and
 // the set's beams into shared memory and compacts the active
@@ -16,6 +16,7 @@
 #include <algorithm>
 #include "rate_core.cuh"
 #include "reduced.cuh"
+#include "kicks.cuh"
 
 namespace {
 
@@ -253,16 +254,16 @@ force_reduced_adjoint_kernel(ForceParams P, double *grad)
                 gf[b * st] = 0.0;
                 gs[b * st] = 0.0;
             }
-            double gB;
+            double gBG;
             const RedOut o = reduced_adjoint_point<NGMAX, NEMAX, EXACT, PAD>(P, S, pol, v, z, Bg, fd, st,
-                                                                             gf, gs, gB);
+                                                                             gf, gs, gBG);
             P.F[gi] = o.F;
             if (P.status) P.status[gi] = o.status;
             for (int b = 0; b < nb; b++) {
                 row[b] = gf[b * st];
                 row[nb + b] = gs[b * st];
             }
-            row[2 * nb] = gB;
+            row[2 * nb] = gBG * (z * 1e4);  // dB/dB' = z 1e4
         }
     }
 }
@@ -454,6 +455,153 @@ traj1d_reduced_kernel(ForceParams P, TrajParams T)
     }
 }
 
+// Trajectory tangents of the per-axis 3D model (molmot/propagation/
+// trajectories.py:78-156: symplectic Euler per axis, F_x = F(v_x, x) at
+// gradient -B'/2, F_y likewise, F_z = F(v_z, z) at B', escape at
+// |r| > r_escape) with respect to parameters theta_k (beam frequency groups,
+// s0 groups, B').  Forward mode; the force's gradient at each step comes from
+// reduced_adjoint_point (FP64-reduced form):
+//   dF_a/dtheta_k = sum_{b: freq_par[b] = k} dF/dfreq_b + sum_{b: s0_par[b] = k} dF/ds0_b
+//                   + [k = B'] dF/dB mult_a x_a 1e4 + dF/dv Tv_ak + dF/dx Tx_ak,
+//   dF/dv = sum_b dF/dfreq_b ck_b / 2pi (ck_b = -k kdir_b),  dF/dx = dF/dB B' mult_a 1e4,
+//   Tv_ak += dt (dF_a/dtheta_k) / m,  Tx_ak += dt Tv_ak,
+// mult_a = -1/2 for x and y, 1 for z.  Recoil kicks (kicks != 0): N ~
+// Poisson((R_x + R_y + R_z) dt) events per step, 2N isotropic kicks of
+// hbar k / m (kicks.cuh, counters (particle, absolute step)); under
+// differentiation they are held fixed (the derivative at fixed noise: event
+// counts and directions do not move with theta).  One particle per thread,
+// the three axes in turn; threads never wait for one another after the
+// prologue.  State row per particle (width 6 + 6 n_par): r[3], v[3],
+// Tr[3][n_par], Tv[3][n_par].
+struct TgParams {
+    double dt, r_escape, mass, v_rec;
+    long long n_particles, n_steps, step0, ckpt_every;
+    int n_par, kicks, bprime_par;
+    unsigned long long seed;
+    signed char freq_par[MM_MAX_BEAMS], s0_par[MM_MAX_BEAMS];
+    double *state;      // [N][6 + 6 n_par], in/out
+    int32_t *n_actual;  // [N], in/out: the absolute step a particle stopped at
+    double *ckpt;       // [n_steps / ckpt_every][N][6 + 6 n_par] or null
+};
+
+constexpr int kTgMaxPar = MM_TGRAD_MAX_PAR;
+constexpr int kTgThreads = 32;
+
+template <int NGMAX, int NEMAX, bool EXACT, int PAD>
+__global__ void __launch_bounds__(kTgThreads)
+traj_grad_kernel(ForceParams P, TgParams T)
+{
+    extern __shared__ __align__(16) unsigned char sm[];
+    RedLayout<NGMAX, NEMAX> Ly;
+    Ly.build(P.n_b);
+    RedView S;
+    build_reduced_tables<NGMAX, NEMAX, PAD, true>(P, 0, sm, Ly, S);
+    const int nb = P.n_b, st = blockDim.x, np = T.n_par, W = 6 + 6 * np;
+    double *fd = (double *)(sm + Ly.total) + threadIdx.x;
+    double *gf = fd + (size_t)nb * st, *gs = gf + (size_t)nb * st;
+    const long long ip = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (ip >= T.n_particles) return;  // after the prologue's barriers
+    const double Bp = P.bgrad[0];
+    double x[3], u[3], Tx[3][kTgMaxPar], Tv[3][kTgMaxPar];
+    double *row = T.state + ip * W;
+    for (int a = 0; a < 3; a++) {
+        x[a] = row[a];
+        u[a] = row[3 + a];
+#pragma unroll
+        for (int k = 0; k < kTgMaxPar; k++) {
+            Tx[a][k] = k < np ? row[6 + a * np + k] : 0.0;
+            Tv[a][k] = k < np ? row[6 + 3 * np + a * np + k] : 0.0;
+        }
+    }
+    auto radius = [&]() {
+        double r2 = 0.0;
+        for (int a = 0; a < 3; a++) r2 = fma(x[a], x[a], r2);
+        return sqrt(r2);
+    };
+    auto write_row = [&](double *dst) {
+        for (int a = 0; a < 3; a++) {
+            dst[a] = x[a];
+            dst[3 + a] = u[a];
+            for (int k = 0; k < np; k++) {
+                dst[6 + a * np + k] = Tx[a][k];
+                dst[6 + 3 * np + a * np + k] = Tv[a][k];
+            }
+        }
+    };
+    // a particle already beyond r_escape stopped in an earlier call
+    const bool stopped = radius() > T.r_escape;
+    long long na = -1;
+    long long n_ck = 0;
+    const long long jend = T.step0 + T.n_steps;
+    long long j = T.step0 + 1;
+    for (; !stopped && j <= jend; j++) {
+        double F[3], dth[3][kTgMaxPar], Rt = 0.0;
+        for (int a = 0; a < 3; a++) {
+            const double mult = (a < 2) ? -0.5 : 1.0;
+            const double Bg = Bp * mult;  // the per-axis model's product (mm_traj_run)
+            for (int b = 0; b < nb; b++) {
+                gf[b * st] = 0.0;
+                gs[b * st] = 0.0;
+            }
+            double gBG;
+            const RedOut o = reduced_adjoint_point<NGMAX, NEMAX, EXACT, PAD>(P, S, P.pol, u[a], x[a], Bg, fd,
+                                                                             st, gf, gs, gBG);
+            F[a] = o.F;
+            Rt += o.R;
+            double dv = 0.0;
+            for (int b = 0; b < nb; b++) dv = fma(gf[b * st], S.ck[b], dv);
+            const double dFdv = dv / MM_TWO_PI, dFdx = gBG * (Bg * 1e4);
+#pragma unroll
+            for (int k = 0; k < kTgMaxPar; k++) dth[a][k] = fma(dFdv, Tv[a][k], dFdx * Tx[a][k]);
+            for (int b = 0; b < nb; b++) {
+                const int kf = T.freq_par[b], ks = T.s0_par[b];
+#pragma unroll
+                for (int k = 0; k < kTgMaxPar; k++) {
+                    if (k == kf) dth[a][k] += gf[b * st];
+                    if (k == ks) dth[a][k] += gs[b * st];
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < kTgMaxPar; k++)
+                if (k == T.bprime_par) dth[a][k] = fma(gBG, mult * x[a] * 1e4, dth[a][k]);
+        }
+        double kick[3] = {0.0, 0.0, 0.0};
+        if (T.kicks) recoil_kick(T.seed, (unsigned)ip, (unsigned)j, Rt * T.dt, T.v_rec, kick);
+        const double im = T.dt / T.mass;
+        for (int a = 0; a < 3; a++) {
+            const double acc = __ddiv_rn(F[a], T.mass);
+            u[a] = __dadd_rn(u[a], __dmul_rn(acc, T.dt));
+            if (T.kicks) u[a] = __dadd_rn(u[a], kick[a]);
+            x[a] = __dadd_rn(x[a], __dmul_rn(u[a], T.dt));
+#pragma unroll
+            for (int k = 0; k < kTgMaxPar; k++) {
+                Tv[a][k] = fma(dth[a][k], im, Tv[a][k]);
+                Tx[a][k] = fma(Tv[a][k], T.dt, Tx[a][k]);
+            }
+        }
+        const bool esc = radius() > T.r_escape;
+        if (T.ckpt && (j - T.step0) % T.ckpt_every == 0) {
+            write_row(T.ckpt + ((size_t)n_ck * T.n_particles + ip) * W);
+            n_ck++;
+        }
+        if (esc) {
+            na = j;
+            j++;
+            break;
+        }
+    }
+    // checkpoints after the particle stopped: the frozen state
+    if (T.ckpt)
+        for (; j <= jend; j++)
+            if ((j - T.step0) % T.ckpt_every == 0) {
+                write_row(T.ckpt + ((size_t)n_ck * T.n_particles + ip) * W);
+                n_ck++;
+            }
+    write_row(row);
+    if (na >= 0) T.n_actual[ip] = (int32_t)na;
+    else if (!stopped) T.n_actual[ip] = (int32_t)jend;
+}
+
 // Size classes: (NGMAX, NEMAX, G, EXACT).
 template <int NGMAX, int NEMAX, int G, bool EXACT>
 struct Class {
@@ -590,6 +738,22 @@ int launch_reduced_adjoint(const ForceParams &P, double *grad, cudaStream_t st)
     return mm_cuda_check(cudaGetLastError(), "force_reduced_adjoint_kernel launch") ? -3 : 0;
 }
 
+template <class C, int PAD>
+int launch_traj_grad(const ForceParams &P, const TgParams &T, cudaStream_t st)
+{
+    auto kern = traj_grad_kernel<C::ng, C::ne, C::exact, PAD>;
+    RedLayout<C::ng, C::ne> Ly;
+    Ly.build(P.n_b);
+    const size_t sb = Ly.total + sizeof(double) * 3 * P.n_b * kTgThreads;
+    if (sb > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb);
+        if (mm_cuda_check(e, "cudaFuncSetAttribute")) return -3;
+    }
+    const long long gx = (T.n_particles + kTgThreads - 1) / kTgThreads;
+    kern<<<(unsigned)gx, kTgThreads, sb, st>>>(P, T);
+    return mm_cuda_check(cudaGetLastError(), "traj_grad_kernel launch") ? -3 : 0;
+}
+
 template <class C>
 int launch_traj(const ForceParams &P, const TrajParams &T, cudaStream_t st)
 {
@@ -631,12 +795,12 @@ int reduced_list_granule(const mm_pack *pack, const mm_beams *beams)
 // checks (the host twin of build_reduced_tables' flags[0]): every ground state
 // has a triple, and the excited chain e' -> e (e' decays to a ground state
 // that a beam of the set excites to e) is strongly connected.
-bool reduced_all_valid(const mm_pack *pack, const mm_beams *beams)
+bool reduced_sets_valid(const mm_pack *pack, const mm_beams *beams, int first, int count)
 {
     const int n_g = pack->n_g, n_e = pack->n_e, n_b = beams->n_b;
     if (n_e > 32) return false;
     std::vector<int> cnt((size_t)n_g * n_e);
-    for (int s = 0; s < beams->n_sets; s++) {
+    for (int s = first; s < first + count; s++) {
         int npol[3] = {0, 0, 0};
         for (int b = 0; b < n_b; b++) npol[beams->h_pol[(size_t)s * n_b + b]]++;
         for (int i = 0; i < n_g * n_e; i++) {
@@ -665,6 +829,11 @@ bool reduced_all_valid(const mm_pack *pack, const mm_beams *beams)
             if ((T[i] & all) != all) return false;
     }
     return true;
+}
+
+bool reduced_all_valid(const mm_pack *pack, const mm_beams *beams)
+{
+    return reduced_sets_valid(pack, beams, 0, beams->n_sets);
 }
 
 // Size-class dispatch.  SrOH (12 ground, 4 excited) has an exact class.
@@ -838,6 +1007,65 @@ extern "C" int mm_traj_run(const mm_pack *pack, const mm_beams *beams, const mm_
         if (!fp32) return launch_traj<CT>(P, T, st);
         return reduced_list_granule(pack, beams) == kRedPad ? launch_traj_reduced<CT, kRedPad>(P, T, st)
                                                             : launch_traj_reduced<CT, 1>(P, T, st);
+    });
+}
+
+extern "C" int mm_traj_grad_run(const mm_pack *pack, const mm_beams *beams, const mm_tgrad_opts *opts,
+                                int64_t n_particles, double *state, int32_t *n_actual, double *ckpt,
+                                void *stream)
+{
+    if (!opts) { mm_set_error("trajectory-gradient options are required"); return -1; }
+    mm_batch_opts bo = {};
+    bo.precision = MM_PREC_FP64_REDUCED;
+    bo.hbar = opts->hbar;
+    ForceParams P;
+    if (fill_params(pack, beams, &bo, P)) return -1;
+    if (n_particles < 0 || opts->n_steps < 0 || opts->step0 < 0) {
+        mm_set_error("n_particles, n_steps and step0 must be >= 0");
+        return -1;
+    }
+    if (opts->step0 + opts->n_steps > 0x7fffffffll) { mm_set_error("step indices exceed 2^31 - 1"); return -1; }
+    if (opts->n_par < 1 || opts->n_par > MM_TGRAD_MAX_PAR) {
+        mm_set_error("n_par=%d out of range [1, %d]", opts->n_par, MM_TGRAD_MAX_PAR);
+        return -1;
+    }
+    for (int b = 0; b < beams->n_b; b++)
+        if (opts->freq_par[b] < -1 || opts->freq_par[b] >= opts->n_par || opts->s0_par[b] < -1 ||
+            opts->s0_par[b] >= opts->n_par) {
+            mm_set_error("beam %d: parameter index out of range [-1, n_par)", b);
+            return -1;
+        }
+    if (opts->bprime_par < -1 || opts->bprime_par >= opts->n_par) {
+        mm_set_error("bprime_par out of range [-1, n_par)");
+        return -1;
+    }
+    if (ckpt && opts->ckpt_every < 1) { mm_set_error("ckpt needs ckpt_every >= 1"); return -1; }
+    if (!reduced_sets_valid(pack, beams, 0, 1)) {
+        mm_set_error("beam set 0 fails the reduced form's structural checks (a ground state no beam "
+                     "pumps, or an excited chain that is not strongly connected)");
+        return -1;
+    }
+    if (n_particles == 0 || opts->n_steps == 0) return 0;
+    if (!state || !n_actual) { mm_set_error("state and n_actual must be non-null"); return -1; }
+    P.layout = MM_LAYOUT_POINTS; P.nv = P.nz = 0; P.pps = 1; P.n_points = 0;
+    P.v = P.z = nullptr; P.F = P.R = P.pop = nullptr; P.status = nullptr;
+    TgParams T;
+    T.dt = opts->dt; T.r_escape = opts->r_escape; T.mass = pack->mass;
+    T.v_rec = P.hbar * P.k / pack->mass;
+    T.n_particles = n_particles; T.n_steps = opts->n_steps; T.step0 = opts->step0;
+    T.ckpt_every = ckpt ? opts->ckpt_every : 0;
+    T.n_par = opts->n_par; T.kicks = opts->kicks ? 1 : 0; T.bprime_par = opts->bprime_par;
+    T.seed = opts->seed;
+    for (int b = 0; b < MM_MAX_BEAMS; b++) {
+        T.freq_par[b] = (signed char)(b < beams->n_b ? opts->freq_par[b] : -1);
+        T.s0_par[b] = (signed char)(b < beams->n_b ? opts->s0_par[b] : -1);
+    }
+    T.state = state; T.n_actual = n_actual; T.ckpt = ckpt;
+    cudaStream_t st = (cudaStream_t)stream;
+    return dispatch_class(P.n_g, P.n_e, [&](auto C) -> int {
+        using CT = decltype(C);
+        return reduced_list_granule(pack, beams) == kRedPad ? launch_traj_grad<CT, kRedPad>(P, T, st)
+                                                            : launch_traj_grad<CT, 1>(P, T, st);
     });
 }
 

@@ -499,18 +499,19 @@ __device__ __forceinline__ RedOut reduced_point(const ForceParams &P, const RedV
 }
 
 // ---------------------------------------------------------------------------
-// Adjoint of the FP64-reduced form: F and dF/d(freq_b, s0_b, B') at one point
-// (one thread).  With u = dF/dpi = (cf - F cw) / norm (u . pi = 0) and lambda
-// solving (I - K)^T lambda = u (lambda_0 = 0: K's columns sum to one, so
-// lambda is defined up to a multiple of the ones vector, which dK annihilates),
+// Adjoint of the FP64-reduced form: F and dF/d(freq_b, s0_b, B) at one point
+// (one thread; B the field in Gauss, B = B' z 1e4).  With
+// u = dF/dpi = (cf - F cw) / norm (u . pi = 0) and lambda solving
+// (I - K)^T lambda = u (lambda_0 = 0: K's columns sum to one, so lambda is
+// defined up to a multiple of the ones vector, which dK annihilates),
 //     dF = sum_g [ y_g sum_e lambda_e d a_ge + (y_g / norm) d phi_g
 //                  - (F y_g / norm) d w_g ],   y_g = sum_e BR[e,g] pi_e,
 // and a_ge, phi_g, w_g are functions of the unsaturated rate sums R_ge, the
 // force sum f_g and the saturation sum s_g.  Each triple (g, b, e) enters
 // those sums through c1 L, hk c1 L and c2 L, so its contribution is
 //     q = alpha_ge c1 + beta_g hk c1 + gamma_g c2   times dL,
-// with dL/dfreq_b = L'(delta) 2 pi, dL/dB' = L'(delta) (-z 1e4 (zd_e - zd_g)
-// Gamma) and d(c1, c2)/ds0_b = (c1, c2) / s0_b written with d2 (s0_b may be 0).
+// with dL/dfreq_b = L'(delta) 2 pi, dL/dB = L'(delta) (-(zd_e - zd_g) Gamma)
+// and d(c1, c2)/ds0_b = (c1, c2) / s0_b written with d2 (s0_b may be 0).
 // gf[b * stride], gs[b * stride]: this thread's per-beam accumulators
 // (shared memory); the caller zeroes them.  pol: the set's polarisations.
 // Valid sets only (S.valid); finite v and z.
@@ -518,7 +519,7 @@ template <int NGMAX, int NEMAX, bool EXACT, int PAD>
 __device__ __forceinline__ RedOut reduced_adjoint_point(const ForceParams &P, const RedView &S,
                                                         const int32_t *pol, double v, double z,
                                                         double Bgrad, double *fd, int stride,
-                                                        double *gf, double *gs, double &gB)
+                                                        double *gf, double *gs, double &gBG)
 {
     const int n_g = EXACT ? NGMAX : P.n_g;
     const int n_e = EXACT ? NEMAX : P.n_e;
@@ -615,7 +616,7 @@ __device__ __forceinline__ RedOut reduced_adjoint_point(const ForceParams &P, co
     lam[0] = 0.0;
 
     // second pass: per ground state coefficients, then the triples once more
-    gB = 0.0;
+    gBG = 0.0;
     const double inrm = in, Fin = F * in;
     for (int g = 0; g < n_g; g++) {
         double Re[NEMAX], f, s;
@@ -640,7 +641,7 @@ __device__ __forceinline__ RedOut reduced_adjoint_point(const ForceParams &P, co
             const double alpha = yi * (lam[e] + common);
             const int i0 = S.offs[g * NEMAX + e], i1 = S.offs[g * NEMAX + e + 1];
             const double om = __dsub_rn(C.Ese[e], Esg);
-            const double dBde = -z * 1e4 * (S.zde[e] - P.zd[g]) * P.Gamma;  // d delta / dB'
+            const double dBde = -(S.zde[e] - P.zd[g]) * P.Gamma;  // d delta / dB
             for (int i = i0; i < i1; i++) {
                 const TripD tr = ((const TripD *)S.trip)[i];
                 if (tr.pad) continue;  // list padding
@@ -655,7 +656,7 @@ __device__ __forceinline__ RedOut reduced_adjoint_point(const ForceParams &P, co
                 const double d2 = P.d2[(g * P.n_e + e) * 3 + pol[b]];
                 const double qs = fma((alpha + beta * tr.hk) * gh * P.geff, d2, gamma * d2);
                 gs[b * stride] = fma(qs, L, gs[b * stride]);
-                gB = fma(q * dLd, dBde, gB);
+                gBG = fma(q * dLd, dBde, gBG);
             }
         }
     }

@@ -27,8 +27,9 @@ def force(mol, kdir, pol, freq, s0, bgrad, v, z, pps, gamma_eff=1.0, hbar=1.0545
     BR = torch.as_tensor(BR, **f64)
     G, k = float(mol.Gamma), float(mol.k)
     gh = G / 2.0
-    v = torch.as_tensor(np.asarray(v), **f64)
-    z = torch.as_tensor(np.asarray(z), **f64)
+    # v, z: arrays, or torch tensors (which may require grad)
+    v = v.to(**f64) if torch.is_tensor(v) else torch.as_tensor(np.asarray(v), **f64)
+    z = z.to(**f64) if torch.is_tensor(z) else torch.as_tensor(np.asarray(z), **f64)
     n = v.numel()
     sid = torch.arange(n, device=dev) // pps
     B = bgrad[sid]
