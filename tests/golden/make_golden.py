@@ -4,7 +4,9 @@
 Run in a container that has the reference checkout (default
 /root/reference, or $MOLMOT_REFERENCE):
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py             # SrOH fixtures
+    python tests/golden/make_golden.py analysis    # analysis_golden.npz
+    python tests/golden/make_golden.py molecules   # molecules_golden.npz (CaF, CaOH)
 
 It (1) extracts the reference's own golden arrays from
 validation/three_way_results.npz and validation/trajectory_cpu_vs_gpu_results.npz,
@@ -233,9 +235,53 @@ def analysis_golden():
     print("analysis golden written")
 
 
+def molecules_golden():
+    """CaF and CaOH (molmot/molecules/caf.py:90, caoh.py:89, built by the
+    reference's own Hamiltonian code): the MolecularData arrays, the derived
+    fields, the reference's DC MOT beams, and _rate_eq_core forces at seeded
+    random points (the 1D path; their ground Zeeman spectra are 6 + 6
+    degenerate like SrOH's, so the 3D model is ill-posed for them too)."""
+    from molmot.molecules.caf import build_caf_hamiltonian
+    from molmot.molecules.caoh import build_caoh_hamiltonian
+    from molmot.obe.fields import LaserBeam, make_dc_mot_beams
+    from molmot.obe.rate_equations_jit import solve_rate_equations_jit
+    out = {"versions": versions()}
+    rng = np.random.default_rng(20261204)
+    for name, build in (("caf", build_caf_hamiltonian), ("caoh", build_caoh_hamiltonian)):
+        m = build(verbose=False)
+        for key in ("energies", "tdm", "zeeman_x", "zeeman_y", "zeeman_z", "d_squared", "zeeman_z_diag"):
+            out[f"{name}_{key}"] = np.asarray(getattr(m, key))
+        for key in ("Gamma", "k", "mass", "wavelength", "n_ground", "n_excited", "omega_J12",
+                    "omega_J32", "omega_mean"):
+            out[f"{name}_{key}"] = np.asarray(getattr(m, key))
+        kd, fr, po, s0 = beams_to_arrays(make_dc_mot_beams(m, delta_Gamma=-0.25, split_Gamma=0.6, s0=1.5))
+        out.update({f"{name}_dc_kdir": kd, f"{name}_dc_freq": fr, f"{name}_dc_pol": po, f"{name}_dc_s0": s0})
+        n_sets, n_pts = 8, 16
+        rows = {k: [] for k in ["kdir", "freq", "pol", "s0", "B", "v", "z", "F", "p", "R"]}
+        for _ in range(n_sets):
+            b = make_dc_mot_beams(m, delta_Gamma=rng.uniform(-3, 0), split_Gamma=rng.uniform(0, 2),
+                                  s0=10 ** rng.uniform(-1, 1))
+            kd, fr, po, s0 = beams_to_arrays(b)
+            fr = fr + np.repeat(rng.uniform(-40e6, 0, 4), 2)
+            s0 = np.repeat(10 ** rng.uniform(-1, 1, 4), 2)
+            b = [LaserBeam(np.array([0.0, 0.0, kd[i]]), fr[i], int(po[i]), s0[i]) for i in range(8)]
+            B = rng.uniform(0.05, 0.4)
+            for _ in range(n_pts):
+                v, zz = rng.uniform(-10, 10), rng.uniform(-1e-2, 1e-2)
+                F, p, R = solve_rate_equations_jit(m, b, v, zz, B)
+                for k, val in zip(rows, [kd, fr, po, s0, B, v, zz, F, p, R]):
+                    rows[k].append(val)
+        out.update({f"{name}_pts_{k}": np.array(v) for k, v in rows.items()})
+        out[f"{name}_n_sets"], out[f"{name}_n_pts"] = n_sets, n_pts
+    np.savez(os.path.join(HERE, "molecules_golden.npz"), **out)
+    print("molecules golden written")
+
+
 if __name__ == "__main__":
     if len(sys.argv) > 1 and sys.argv[1] == "analysis":
         analysis_golden()
+    elif len(sys.argv) > 1 and sys.argv[1] == "molecules":
+        molecules_golden()
     else:
         main()
         analysis_golden()
