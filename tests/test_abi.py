@@ -75,3 +75,34 @@ def test_force_batch_rejects_null_handles():
     rc = L.mm_force_batch(None, None, None, None, 1, ctypes.byref(o), None, None, None, None, None)
     assert rc < 0
     assert b"null" in L.mm_last_error()
+
+
+def test_option_struct_layouts_match_header(tmp_path):
+    """Every ctypes mirror of a header struct has the C compiler's size and
+    field offsets (gcc on a probe that includes the header)."""
+    import shutil
+    import subprocess
+    from molmot_b200 import _lib
+    if shutil.which("gcc") is None:
+        pytest.skip("gcc not available")
+    pairs = [("mm_mol_desc", _lib.MolDesc), ("mm_beam_desc", _lib.BeamDesc),
+             ("mm_batch_opts", _lib.BatchOpts), ("mm_traj_opts", _lib.TrajOpts),
+             ("mm_uneven_opts", _lib.UnevenOpts), ("mm_tgrad_opts", _lib.TgradOpts)]
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "molmot_b200.h"', "int main(void) {"]
+    for cname, cls in pairs:
+        lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
+        for fname, _ in cls._fields_:
+            lines.append(f'  printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "probe.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "probe"
+    subprocess.run(["gcc", "-std=c11", "-I", os.path.dirname(HEADER), str(src), "-o", str(exe)], check=True)
+    got = {}
+    for ln in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.splitlines():
+        a, b, c = ln.split()
+        got[(a, b)] = int(c)
+    for cname, cls in pairs:
+        assert got[(cname, "size")] == ctypes.sizeof(cls), cname
+        for fname, _ in cls._fields_:
+            assert got[(cname, fname)] == getattr(cls, fname).offset, (cname, fname)

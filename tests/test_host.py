@@ -81,3 +81,19 @@ def test_reference_simulator_objects_adapt(mol):
     assert isinstance(g, RFMOTSimulator)
     (b0, B0), (b1, B1) = g.param_sets()
     assert B0 == -B1 and [x.polarization for x in b0] != [x.polarization for x in b1]
+
+
+def test_trajectory_gradient_parameter_maps():
+    """Host-side checks of mm_traj_grad_run's parameter maps (no GPU)."""
+    from molmot_b200 import _lib
+    from molmot_b200.trajgrad import _param_map
+    m = _param_map([0, 0, 1, 1, -1, -1, 2, 2], 8, 3, "freq_par")
+    assert list(m)[:8] == [0, 0, 1, 1, -1, -1, 2, 2] and all(x == -1 for x in list(m)[8:])
+    assert len(m) == _lib.MM_MAX_BEAMS
+    assert all(x == -1 for x in _param_map(None, 8, 3, "s0_par"))
+    with pytest.raises(ValueError):
+        _param_map([0, 3], 2, 3, "freq_par")       # index beyond n_par
+    with pytest.raises(ValueError):
+        _param_map([0, 1, 2], 2, 3, "freq_par")    # one entry per beam
+    import ctypes
+    assert ctypes.sizeof(_lib.TgradOpts) == 8 * 7 + 4 * 2 + 4 * 2 * _lib.MM_MAX_BEAMS + 4 * 2
