@@ -469,10 +469,12 @@ traj1d_reduced_kernel(ForceParams P, TrajParams T)
 // Poisson((R_x + R_y + R_z) dt) events per step, 2N isotropic kicks of
 // hbar k / m (kicks.cuh, counters (particle, absolute step)); under
 // differentiation they are held fixed (the derivative at fixed noise: event
-// counts and directions do not move with theta).  One particle per thread,
-// the three axes in turn; threads never wait for one another after the
-// prologue.  State row per particle (width 6 + 6 n_par): r[3], v[3],
-// Tr[3][n_par], Tv[3][n_par].
+// counts and directions do not move with theta).  Four lanes per particle:
+// lane a < 3 integrates axis a, lane 3 only joins the sums.  The lanes of a
+// particle share the kick's total rate and the escape radius through
+// shuffles that every lane of the warp executes unconditionally, including
+// lanes without a particle and particles that stopped.  State row per
+// particle (width 6 + 6 n_par): r[3], v[3], Tr[3][n_par], Tv[3][n_par].
 struct TgParams {
     double dt, r_escape, mass, v_rec;
     long long n_particles, n_steps, step0, ckpt_every;
@@ -485,10 +487,10 @@ struct TgParams {
 };
 
 constexpr int kTgMaxPar = MM_TGRAD_MAX_PAR;
-constexpr int kTgThreads = 32;
+constexpr int kTgThreads = 128;
 
 template <int NGMAX, int NEMAX, bool EXACT, int PAD>
-__global__ void __launch_bounds__(kTgThreads)
+__global__ void __launch_bounds__(kTgThreads, 2)
 traj_grad_kernel(ForceParams P, TgParams T)
 {
     extern __shared__ __align__(16) unsigned char sm[];
@@ -499,107 +501,116 @@ traj_grad_kernel(ForceParams P, TgParams T)
     const int nb = P.n_b, st = blockDim.x, np = T.n_par, W = 6 + 6 * np;
     double *fd = (double *)(sm + Ly.total) + threadIdx.x;
     double *gf = fd + (size_t)nb * st, *gs = gf + (size_t)nb * st;
-    const long long ip = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (ip >= T.n_particles) return;  // after the prologue's barriers
-    const double Bp = P.bgrad[0];
-    double x[3], u[3], Tx[3][kTgMaxPar], Tv[3][kTgMaxPar];
-    double *row = T.state + ip * W;
-    for (int a = 0; a < 3; a++) {
-        x[a] = row[a];
-        u[a] = row[3 + a];
+    const int a = threadIdx.x & 3;
+    const bool axis = a < 3;
+    const long long ip = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 2;
+    const bool valid = ip < T.n_particles;
+    const double mult = (a < 2) ? -0.5 : 1.0;
+    const double Bg = P.bgrad[0] * mult;  // the per-axis model's product (mm_traj_run)
+    double x = 0.0, u = 0.0, Tx[kTgMaxPar], Tv[kTgMaxPar];
+    double *row = T.state + (valid ? ip : 0) * W;
 #pragma unroll
-        for (int k = 0; k < kTgMaxPar; k++) {
-            Tx[a][k] = k < np ? row[6 + a * np + k] : 0.0;
-            Tv[a][k] = k < np ? row[6 + 3 * np + a * np + k] : 0.0;
-        }
+    for (int k = 0; k < kTgMaxPar; k++) {
+        const bool on = valid && axis && k < np;
+        Tx[k] = on ? row[6 + a * np + k] : 0.0;
+        Tv[k] = on ? row[6 + 3 * np + a * np + k] : 0.0;
     }
-    auto radius = [&]() {
-        double r2 = 0.0;
-        for (int a = 0; a < 3; a++) r2 = fma(x[a], x[a], r2);
-        return sqrt(r2);
-    };
+    if (valid && axis) {
+        x = row[a];
+        u = row[3 + a];
+    }
     auto write_row = [&](double *dst) {
-        for (int a = 0; a < 3; a++) {
-            dst[a] = x[a];
-            dst[3 + a] = u[a];
+        if (valid && axis) {
+            dst[a] = x;
+            dst[3 + a] = u;
             for (int k = 0; k < np; k++) {
-                dst[6 + a * np + k] = Tx[a][k];
-                dst[6 + 3 * np + a * np + k] = Tv[a][k];
+                dst[6 + a * np + k] = Tx[k];
+                dst[6 + 3 * np + a * np + k] = Tv[k];
             }
         }
     };
-    // a particle already beyond r_escape stopped in an earlier call
-    const bool stopped = radius() > T.r_escape;
+    // a particle already beyond r_escape stopped in an earlier call (the sum
+    // runs on every lane: it is a warp collective)
+    const double r2_0 = mm_group_sum(x * x, 4);
+    const bool stopped = !valid || sqrt(r2_0) > T.r_escape;
+    bool done = stopped;
     long long na = -1;
     long long n_ck = 0;
     const long long jend = T.step0 + T.n_steps;
     long long j = T.step0 + 1;
-    for (; !stopped && j <= jend; j++) {
-        double F[3], dth[3][kTgMaxPar], Rt = 0.0;
-        for (int a = 0; a < 3; a++) {
-            const double mult = (a < 2) ? -0.5 : 1.0;
-            const double Bg = Bp * mult;  // the per-axis model's product (mm_traj_run)
+    for (; j <= jend; j++) {
+        if (__all_sync(0xffffffffu, done)) break;
+        double F = 0.0, R = 0.0, dth[kTgMaxPar];
+#pragma unroll
+        for (int k = 0; k < kTgMaxPar; k++) dth[k] = 0.0;
+        if (!done && axis) {
             for (int b = 0; b < nb; b++) {
                 gf[b * st] = 0.0;
                 gs[b * st] = 0.0;
             }
             double gBG;
-            const RedOut o = reduced_adjoint_point<NGMAX, NEMAX, EXACT, PAD>(P, S, P.pol, u[a], x[a], Bg, fd,
-                                                                             st, gf, gs, gBG);
-            F[a] = o.F;
-            Rt += o.R;
+            const RedOut o = reduced_adjoint_point<NGMAX, NEMAX, EXACT, PAD>(P, S, P.pol, u, x, Bg, fd, st,
+                                                                             gf, gs, gBG);
+            F = o.F;
+            R = o.R;
             double dv = 0.0;
             for (int b = 0; b < nb; b++) dv = fma(gf[b * st], S.ck[b], dv);
             const double dFdv = dv / MM_TWO_PI, dFdx = gBG * (Bg * 1e4);
 #pragma unroll
-            for (int k = 0; k < kTgMaxPar; k++) dth[a][k] = fma(dFdv, Tv[a][k], dFdx * Tx[a][k]);
+            for (int k = 0; k < kTgMaxPar; k++) dth[k] = fma(dFdv, Tv[k], dFdx * Tx[k]);
             for (int b = 0; b < nb; b++) {
                 const int kf = T.freq_par[b], ks = T.s0_par[b];
 #pragma unroll
                 for (int k = 0; k < kTgMaxPar; k++) {
-                    if (k == kf) dth[a][k] += gf[b * st];
-                    if (k == ks) dth[a][k] += gs[b * st];
+                    if (k == kf) dth[k] += gf[b * st];
+                    if (k == ks) dth[k] += gs[b * st];
                 }
             }
 #pragma unroll
             for (int k = 0; k < kTgMaxPar; k++)
-                if (k == T.bprime_par) dth[a][k] = fma(gBG, mult * x[a] * 1e4, dth[a][k]);
+                if (k == T.bprime_par) dth[k] = fma(gBG, mult * x * 1e4, dth[k]);
         }
+        // warp collectives below: every lane, every iteration
         double kick[3] = {0.0, 0.0, 0.0};
-        if (T.kicks) recoil_kick(T.seed, (unsigned)ip, (unsigned)j, Rt * T.dt, T.v_rec, kick);
-        const double im = T.dt / T.mass;
-        for (int a = 0; a < 3; a++) {
-            const double acc = __ddiv_rn(F[a], T.mass);
-            u[a] = __dadd_rn(u[a], __dmul_rn(acc, T.dt));
-            if (T.kicks) u[a] = __dadd_rn(u[a], kick[a]);
-            x[a] = __dadd_rn(x[a], __dmul_rn(u[a], T.dt));
+        if (T.kicks) {  // uniform over the grid
+            const double Rt = (R + __shfl_xor_sync(0xffffffffu, R, 1)) +
+                              (__shfl_xor_sync(0xffffffffu, R, 2) + __shfl_xor_sync(0xffffffffu, R, 3));
+            if (!done) recoil_kick(T.seed, (unsigned)ip, (unsigned)j, Rt * T.dt, T.v_rec, kick);
+        }
+        if (!done && axis) {
+            const double acc = __ddiv_rn(F, T.mass);
+            u = __dadd_rn(u, __dmul_rn(acc, T.dt));
+            if (T.kicks) u = __dadd_rn(u, kick[a]);
+            x = __dadd_rn(x, __dmul_rn(u, T.dt));
+            const double im = T.dt / T.mass;
 #pragma unroll
             for (int k = 0; k < kTgMaxPar; k++) {
-                Tv[a][k] = fma(dth[a][k], im, Tv[a][k]);
-                Tx[a][k] = fma(Tv[a][k], T.dt, Tx[a][k]);
+                Tv[k] = fma(dth[k], im, Tv[k]);
+                Tx[k] = fma(Tv[k], T.dt, Tx[k]);
             }
         }
-        const bool esc = radius() > T.r_escape;
+        const double r2 = mm_group_sum(x * x, 4);
+        if (!done && sqrt(r2) > T.r_escape) {
+            na = j;
+            done = true;
+        }
         if (T.ckpt && (j - T.step0) % T.ckpt_every == 0) {
-            write_row(T.ckpt + ((size_t)n_ck * T.n_particles + ip) * W);
+            write_row(T.ckpt + ((size_t)n_ck * T.n_particles + (valid ? ip : 0)) * W);
             n_ck++;
         }
-        if (esc) {
-            na = j;
-            j++;
-            break;
-        }
     }
-    // checkpoints after the particle stopped: the frozen state
+    // checkpoints after the whole warp stopped: the frozen state
     if (T.ckpt)
         for (; j <= jend; j++)
             if ((j - T.step0) % T.ckpt_every == 0) {
-                write_row(T.ckpt + ((size_t)n_ck * T.n_particles + ip) * W);
+                write_row(T.ckpt + ((size_t)n_ck * T.n_particles + (valid ? ip : 0)) * W);
                 n_ck++;
             }
     write_row(row);
-    if (na >= 0) T.n_actual[ip] = (int32_t)na;
-    else if (!stopped) T.n_actual[ip] = (int32_t)jend;
+    if (valid && a == 0) {
+        if (na >= 0) T.n_actual[ip] = (int32_t)na;
+        else if (!stopped) T.n_actual[ip] = (int32_t)jend;
+    }
 }
 
 // Size classes: (NGMAX, NEMAX, G, EXACT).
@@ -749,7 +760,7 @@ int launch_traj_grad(const ForceParams &P, const TgParams &T, cudaStream_t st)
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb);
         if (mm_cuda_check(e, "cudaFuncSetAttribute")) return -3;
     }
-    const long long gx = (T.n_particles + kTgThreads - 1) / kTgThreads;
+    const long long gx = (4 * T.n_particles + kTgThreads - 1) / kTgThreads;
     kern<<<(unsigned)gx, kTgThreads, sb, st>>>(P, T);
     return mm_cuda_check(cudaGetLastError(), "traj_grad_kernel launch") ? -3 : 0;
 }
