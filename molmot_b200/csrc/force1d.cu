@@ -918,9 +918,9 @@ static int prepare_batch(const mm_pack *pack, const mm_beams *beams, const doubl
 {
     if (fill_params(pack, beams, opts, P)) return -1;
     if (!opts) { mm_set_error("opts is required"); return -1; }
-    if (!v || !z || !F) { mm_set_error("v, z and F must be non-null"); return -1; }
     if (n_points < 0) { mm_set_error("n_points < 0"); return -1; }
-    if (n_points == 0) return 0;
+    if (n_points == 0) return 0;  // an empty batch may pass null arrays
+    if (!v || !z || !F) { mm_set_error("v, z and F must be non-null"); return -1; }
     P.layout = opts->layout;
     P.nv = opts->nv; P.nz = opts->nz; P.pps = opts->points_per_set;
     if (opts->layout == MM_LAYOUT_GRID) {
@@ -985,7 +985,7 @@ extern "C" int mm_traj_run(const mm_pack *pack, const mm_beams *beams, const mm_
     bo.hbar = topt->hbar;
     ForceParams P;
     if (fill_params(pack, beams, &bo, P)) return -1;
-    if (!r0 || !v0 || !r_final || !v_final || !n_actual) {
+    if (n_particles > 0 && (!r0 || !v0 || !r_final || !v_final || !n_actual)) {
         mm_set_error("r0, v0, r_final, v_final and n_actual must be non-null");
         return -1;
     }

@@ -626,9 +626,9 @@ extern "C" int mm_force3d_batch(const mm_pack *pack, const mm_beams *beams, cons
 {
     Force3Params P;
     if (fill3(pack, beams, hbar, 1, P)) return -1;
-    if (!r || !v || !F) { mm_set_error("r, v and F must be non-null"); return -1; }
     if (n_points < 0) { mm_set_error("n_points < 0"); return -1; }
-    if (n_points == 0) return 0;
+    if (n_points == 0) return 0;  // an empty batch may pass null arrays
+    if (!r || !v || !F) { mm_set_error("r, v and F must be non-null"); return -1; }
     const long long pps = points_per_set > 0 ? points_per_set : n_points;
     if ((n_points + pps - 1) / pps > beams->n_sets) {
         mm_set_error("%lld points at %lld per set need more than %d sets", (long long)n_points, pps,
@@ -660,7 +660,7 @@ extern "C" int mm_traj3d_run(const mm_pack *pack, const mm_beams *beams, const d
 {
     Force3Params P;
     if (fill3(pack, beams, hbar, 1, P)) return -1;
-    if (!r0 || !v0 || !r_out || !vh_out || !n_actual) {
+    if (n_particles > 0 && (!r0 || !v0 || !r_out || !vh_out || !n_actual)) {
         mm_set_error("r0, v0, r_out, vh_out and n_actual must be non-null");
         return -1;
     }
