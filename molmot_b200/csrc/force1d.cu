@@ -10,8 +10,9 @@
 //    groups of G = 4 lanes per point, the reference's elimination
 //    (rate_core.cuh); the trajectory kernel runs a particle per group.
 //  * FP32-bulk and FP64-reduced forms (force_reduced_kernel,
-//    traj1d_reduced_kernel): one point or particle per thread, populations
-//    from the excited-state chain (reduced.cuh).
+//    traj1d_reduced_kernel): one point or particle per thread (two points
+//    per thread for FP32 force maps without populations), populations from
+//    the excited-state chain (reduced.cuh).
 #include <stdio.h>
 #include <algorithm>
 #include "rate_core.cuh"
@@ -156,9 +157,12 @@ force_adjoint_kernel(ForceParams P, double *grad)
 #endif
 
 constexpr int kRedThreads = MM_RED_THREADS;
+// The FP32 form's two-point path needs ~166 registers: 3 CTAs per SM
+// (24.0 ms per 2.68e8 points, against 27.3 ms for one point per thread at 4).
+constexpr int kRedMinBlocks32 = 3;
 
 template <int NGMAX, int NEMAX, bool EXACT, int PAD, bool F64>
-__global__ void __launch_bounds__(kRedThreads, MM_RED_MINB)
+__global__ void __launch_bounds__(kRedThreads, F64 ? MM_RED_MINB : kRedMinBlocks32)
 force_reduced_kernel(ForceParams P)
 {
     extern __shared__ __align__(16) unsigned char sm[];
@@ -179,6 +183,45 @@ force_reduced_kernel(ForceParams P)
         const long long start = (long long)blockIdx.x * chunk;
         const long long end = min(start + chunk, set_count);
         const bool idx32 = P.layout == MM_LAYOUT_GRID && end <= 0x7fffffffll;
+        if constexpr (!F64) {
+            // FP32 form without populations: two points per thread (ip, ip + blockDim.x)
+            if (!P.pop && S.valid) {
+                auto load = [&](long long ip, double &v, double &z) {
+                    if (P.layout == MM_LAYOUT_GRID) {
+                        v = P.v[ip / P.nz];
+                        z = P.z[ip % P.nz];
+                    } else {
+                        v = P.v[set_first + ip];
+                        z = P.z[set_first + ip];
+                    }
+                };
+                for (long long ip0 = start + threadIdx.x; ip0 < end; ip0 += 2 * blockDim.x) {
+                    const long long ip1 = ip0 + blockDim.x;
+                    double v[2], z[2];
+                    load(ip0, v[0], z[0]);
+                    const bool two = ip1 < end;
+                    if (two) load(ip1, v[1], z[1]);
+                    if (two && isfinite(v[0]) && isfinite(z[0]) && isfinite(v[1]) && isfinite(z[1])) {
+                        RedOut o[2];
+                        reduced_point2<NGMAX, NEMAX, EXACT, PAD>(P, S, v, z, Bg, o);
+                        P.F[set_first + ip0] = o[0].F;
+                        P.F[set_first + ip1] = o[1].F;
+                        if (P.R) { P.R[set_first + ip0] = o[0].R; P.R[set_first + ip1] = o[1].R; }
+                        if (P.status) { P.status[set_first + ip0] = o[0].status; P.status[set_first + ip1] = o[1].status; }
+                    } else {
+                        for (int h = 0; h < (two ? 2 : 1); h++) {
+                            const long long gi = set_first + (h ? ip1 : ip0);
+                            const RedOut o = reduced_point<NGMAX, NEMAX, EXACT, PAD, F64>(P, S, v[h], z[h], Bg,
+                                                                                           nullptr, fd, blockDim.x);
+                            P.F[gi] = o.F;
+                            if (P.R) P.R[gi] = o.R;
+                            if (P.status) P.status[gi] = o.status;
+                        }
+                    }
+                }
+                continue;
+            }
+        }
         for (long long ip = start + threadIdx.x; ip < end; ip += blockDim.x) {
             double v, z;
             if (idx32) {  // 32-bit division for grids below 2^31 points per set

@@ -498,6 +498,94 @@ __device__ __forceinline__ RedOut reduced_point(const ForceParams &P, const RedV
     return o;
 }
 
+// Two points of the FP32 form at once (finite inputs, valid set): each triple
+// record is read once for both, and the two points' Lorentzian chains give
+// the scheduler independent work; per point the operations are those of
+// reduced_point, so the results are the same bits.
+template <int NGMAX, int NEMAX, bool EXACT, int PAD>
+__device__ __forceinline__ void reduced_point2(const ForceParams &P, const RedView &S, const double *v,
+                                               const double *z, double Bgrad, RedOut *o)
+{
+    const int n_g = EXACT ? NGMAX : P.n_g;
+    const int n_e = EXACT ? NEMAX : P.n_e;
+    float vf[2], Bf[2];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        const double B = __dmul_rn(__dmul_rn(Bgrad, z[h]), 1e4);
+        vf[h] = (float)v[h];
+        Bf[h] = (float)B;
+    }
+    double K[2][NEMAX][NEMAX], cw[2][NEMAX], cf[2][NEMAX];
+#pragma unroll
+    for (int h = 0; h < 2; h++)
+#pragma unroll
+        for (int e = 0; e < NEMAX; e++) {
+            cw[h][e] = 0.0;
+            cf[h][e] = 0.0;
+#pragma unroll
+            for (int e2 = 0; e2 < NEMAX; e2++) K[h][e][e2] = 0.0;
+        }
+    for (int g = 0; g < n_g; g++) {
+        double Re[2][NEMAX], f[2] = {0.0, 0.0};
+        float sat[2] = {0.0f, 0.0f};
+#pragma unroll
+        for (int e = 0; e < NEMAX; e++) {
+            double acc[2] = {0.0, 0.0};
+            const int i1 = S.offs[g * NEMAX + e + 1];
+#pragma unroll 1
+            for (int i = S.offs[g * NEMAX + e]; i < i1; i += PAD) {
+#pragma unroll
+                for (int j = 0; j < PAD; j++) {
+                    const TripR tr = ((const TripR *)S.trip)[i + j];
+                    reduced_triple(tr, vf[0], Bf[0], acc[0], f[0], sat[0]);
+                    reduced_triple(tr, vf[1], Bf[1], acc[1], f[1], sat[1]);
+                }
+            }
+            Re[0][e] = acc[0];
+            Re[1][e] = acc[1];
+        }
+        double br[NEMAX];
+#pragma unroll
+        for (int e = 0; e < NEMAX; e++) br[e] = S.brt[g * NEMAX + e];
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            double rt = 0.0;
+#pragma unroll
+            for (int e = 0; e < NEMAX; e++) rt += Re[h][e];
+            const double inv = mm_rcp(rt);
+            const double phi = f[h] * inv;
+            const double w = (1.0 + (double)sat[h]) * inv;
+#pragma unroll
+            for (int e = 0; e < NEMAX; e++) {
+                const double a = Re[h][e] * inv;
+#pragma unroll
+                for (int e2 = 0; e2 < NEMAX; e2++) K[h][e][e2] = fma(a, br[e2], K[h][e][e2]);
+            }
+#pragma unroll
+            for (int e = 0; e < NEMAX; e++) {
+                cw[h][e] = fma(br[e], w, cw[h][e]);
+                cf[h][e] = fma(br[e], phi, cf[h][e]);
+            }
+        }
+    }
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        double pi[NEMAX];
+        const bool ok = gth_stationary<NEMAX>(K[h], n_e, pi);
+        double nrm = 0.0, fn = 0.0, rn = 0.0;
+#pragma unroll
+        for (int e = 0; e < NEMAX; e++) {
+            nrm = fma(cw[h][e], pi[e], nrm);
+            fn = fma(cf[h][e], pi[e], fn);
+            rn = fma(S.rsum[e], pi[e], rn);
+        }
+        const double in = mm_rcp(nrm);
+        o[h].F = fn * in;
+        o[h].R = rn * in;
+        o[h].status = (!ok || !isfinite(o[h].F)) ? MM_ST_NONFINITE : 0;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Adjoint of the FP64-reduced form: F and dF/d(freq_b, s0_b, B) at one point
 // (one thread; B the field in Gauss, B = B' z 1e4).  With

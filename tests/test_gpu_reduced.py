@@ -213,3 +213,34 @@ def test_fp64_reduced_form_matches_plain(mol, pack):
     b = force_batch(pack, dark, v[::8], z[::8], grid=True, precision="fp64")
     assert np.max(np.abs(a["pop"].cpu().numpy() - b["pop"].cpu().numpy())) < 1e-12
     assert np.array_equal(a["status"].cpu().numpy(), b["status"].cpu().numpy())
+
+
+def test_fp32_two_point_path_equals_one_point_path(mol, pack):
+    """Without populations the FP32 kernel solves two points per thread; with
+    them, one.  Same bits, including a ragged last pair, a structurally
+    invalid set and non-finite points (which take the one-point path)."""
+    import bench
+    from molmot_b200.engine import BeamSets, force_batch
+    kdir, freq, pol, s0, B = bench.make_params(mol, 5, 77)
+    pol = pol.copy()
+    pol[3] = 1  # all beams pi: ground state 11 unpumped, the elimination path
+    bs = BeamSets(kdir, freq, pol, s0, B)
+    rng = np.random.default_rng(78)
+    npt = 389  # odd, not a multiple of the CTA size
+    v = rng.uniform(-10, 10, 5 * npt)
+    z = rng.uniform(-1e-2, 1e-2, 5 * npt)
+    v[[7, 400, 1201]] = [np.nan, np.inf, 0.3]
+    z[[7, 400, 1201]] = [0.0, 1e-3, np.nan]
+    a = force_batch(pack, bs, v, z, points_per_set=npt, precision="fp32", want_pop=False)
+    b = force_batch(pack, bs, v, z, points_per_set=npt, precision="fp32", want_pop=True)
+    fa, fb = a["F"].cpu().numpy(), b["F"].cpu().numpy()
+    assert np.array_equal(np.isnan(fa), np.isnan(fb))
+    ok = ~np.isnan(fb)
+    assert np.array_equal(fa[ok], fb[ok])
+    assert np.array_equal(a["R"].cpu().numpy()[ok], b["R"].cpu().numpy()[ok])
+    assert np.array_equal(a["status"].cpu().numpy(), b["status"].cpu().numpy())
+    g = force_batch(pack, bs, np.linspace(-10, 10, 37), np.linspace(-1e-2, 1e-2, 29), grid=True,
+                    precision="fp32", want_pop=False)["F"].cpu().numpy()
+    h = force_batch(pack, bs, np.linspace(-10, 10, 37), np.linspace(-1e-2, 1e-2, 29), grid=True,
+                    precision="fp32")["F"].cpu().numpy()
+    assert np.array_equal(g, h)
