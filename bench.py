@@ -147,9 +147,9 @@ def peak_probe(torch):
     return out
 
 
-def cpu_baseline(mol, n_sets_sample=1024):
+def cpu_baseline(mol, n_sets_sample=2048):
     """The reference's numba core (restated) on all host cores, on a sample of
-    1024 of the 4096 parameter sets (6.7e7 points, about 12 s on 16 cores)."""
+    2048 of the 4096 parameter sets (1.3e8 points, about 15 s on 16 cores)."""
     from oracle import rate_eq_numba as nb
     kdir, freq, pol, s0, B = make_params(mol, n_sets_sample, SEED)
     v = np.linspace(-10, 10, NV)
