@@ -187,7 +187,12 @@ force_reduced_kernel(ForceParams P)
             // FP32 form without populations: two points per thread (ip, ip + blockDim.x)
             if (!P.pop && S.valid) {
                 auto load = [&](long long ip, double &v, double &z) {
-                    if (P.layout == MM_LAYOUT_GRID) {
+                    if (idx32) {  // 32-bit division for grids below 2^31 points per set
+                        const unsigned iu = (unsigned)ip, nz = (unsigned)P.nz;
+                        const unsigned iv = iu / nz;
+                        v = P.v[iv];
+                        z = P.z[iu - iv * nz];
+                    } else if (P.layout == MM_LAYOUT_GRID) {
                         v = P.v[ip / P.nz];
                         z = P.z[ip % P.nz];
                     } else {
