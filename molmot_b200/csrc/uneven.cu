@@ -79,13 +79,17 @@ template <int NGMAX, int NEMAX, bool RED = false>
 struct ULayout {
     static constexpr int LDA = NGMAX + 1;
     static constexpr int LDK = NEMAX + 1;
+    // row stride of the rates Rm[g][e]: lanes own consecutive ground states,
+    // so an odd stride keeps their row accesses in distinct banks (the
+    // elimination layout keeps NEMAX; its matrix is the larger footprint)
+    static constexpr int LDR = RED ? NEMAX + 1 : NEMAX;
     // per CTA
     static constexpr int mol_doubles = 2 * (NGMAX + NEMAX) + NGMAX * NEMAX * 3 + NEMAX * NGMAX + NGMAX;
     static constexpr int beam_doubles = 5 * NBU;
     // per group
     // elimination: A, Rm, bv, xv, invU, Fk, Rk, Esg, fd, Ese
     // reduced:     Rm (scaled rates), K, Fk, Rk, Esg, w, phi, fd, Ese, cw, cf, rs, pi
-    static constexpr int grp_raw = RED ? NGMAX * NEMAX + NEMAX * LDK + 5 * NGMAX + NBU + 5 * NEMAX
+    static constexpr int grp_raw = RED ? NGMAX * LDR + NEMAX * LDK + 5 * NGMAX + NBU + 5 * NEMAX
                                        : NGMAX * LDA + NGMAX * NEMAX + 6 * NGMAX + NBU + NEMAX;
     // two 16-lane groups of a warp read the same offsets of their own region:
     // a stride of 16 banks past a multiple of 128 bytes keeps those reads
@@ -114,7 +118,7 @@ __global__ void __launch_bounds__(256)
 uneven_kernel(UnevenParams P)
 {
     using Ly = ULayout<NGMAX, NEMAX, RED>;
-    constexpr int LDA = Ly::LDA, LDK = Ly::LDK;
+    constexpr int LDA = Ly::LDA, LDK = Ly::LDK, LDR = Ly::LDR;
     extern __shared__ __align__(16) unsigned char smraw[];
     double *smd = (double *)smraw;
     // molecule
@@ -134,12 +138,12 @@ uneven_kernel(UnevenParams P)
     double *Kc = nullptr, *wg = nullptr, *ph = nullptr, *cw = nullptr, *cf = nullptr, *rsv = nullptr,
            *piv = nullptr;
     if constexpr (RED) {
-        Rm = W; Kc = Rm + NGMAX * NEMAX; Fk = Kc + NEMAX * LDK; Rk = Fk + NGMAX; Esg = Rk + NGMAX;
+        Rm = W; Kc = Rm + NGMAX * LDR; Fk = Kc + NEMAX * LDK; Rk = Fk + NGMAX; Esg = Rk + NGMAX;
         wg = Esg + NGMAX; ph = wg + NGMAX; fd = ph + NGMAX; Ese = fd + NBU;
         cw = Ese + NEMAX; cf = cw + NEMAX; rsv = cf + NEMAX; piv = rsv + NEMAX;
         A = bv = xv = invU = nullptr;
     } else {
-        A = W; Rm = A + NGMAX * LDA; bv = Rm + NGMAX * NEMAX; xv = bv + NGMAX;
+        A = W; Rm = A + NGMAX * LDA; bv = Rm + NGMAX * LDR; xv = bv + NGMAX;
         invU = xv + NGMAX; Fk = invU + NGMAX; Rk = Fk + NGMAX; Esg = Rk + NGMAX;
         fd = Esg + NGMAX; Ese = fd + NBU;
     }
@@ -159,8 +163,18 @@ uneven_kernel(UnevenParams P)
         const double Gam = P.gam[m], kw = P.kw[m];
         const double *mb = P.buf + P.off[m];
         for (int i = threadIdx.x; i < n_s; i += blockDim.x) { E[i] = mb[i]; zd[i] = mb[n_s + i]; }
-        for (int i = threadIdx.x; i < n_g * n_e * 3; i += blockDim.x) d2s[i] = mb[2 * n_s + i];
-        for (int i = threadIdx.x; i < n_e * n_g; i += blockDim.x) BR[i] = mb[2 * n_s + n_g * n_e * 3 + i];
+        // |d|^2 transposed to [e][q][g]: the lanes of a group own consecutive
+        // ground states, so their reads of one (e, q) are consecutive doubles
+        for (int i = threadIdx.x; i < n_g * n_e * 3; i += blockDim.x) {
+            const int k = i / (n_e * 3), r = i - k * (n_e * 3);
+            d2s[r * NGMAX + k] = mb[2 * n_s + i];  // r = e * 3 + q
+        }
+        // branching ratios transposed to [g][e]: the chain build's lanes read
+        // consecutive excited states of one ground state
+        for (int i = threadIdx.x; i < n_e * n_g; i += blockDim.x) {
+            const int e = i / n_g, g = i - e * n_g;
+            BR[g * NEMAX + e] = mb[2 * n_s + n_g * n_e * 3 + i];
+        }
         for (int i = threadIdx.x; i < n_g; i += blockDim.x) czd[i] = mb[n_s + i] * Gam / MM_TWO_PI;
         const double gh = Gam / 2.0, gh2 = gh * gh;
         for (int b = threadIdx.x; b < n_b; b += blockDim.x) {
@@ -202,7 +216,7 @@ uneven_kernel(UnevenParams P)
 #pragma unroll
                     for (int e = 0; e < NEMAX; e++) {
                         if (e >= n_e) break;
-                        const double d2 = d2s[(k * n_e + e) * 3 + q];
+                        const double d2 = d2s[(e * 3 + q) * NGMAX + k];
                         if (d2 < 1e-15) continue;
                         const double om = __dsub_rn(Ese[e], Eg);
                         const double de = __dmul_rn(__dsub_rn(fdb, om), MM_TWO_PI);
@@ -219,7 +233,7 @@ uneven_kernel(UnevenParams P)
                 for (int e = 0; e < NEMAX; e++) {
                     if (e < n_e) {
                         const double r = Racc[e] * sat;
-                        Rm[k * NEMAX + e] = r;
+                        Rm[k * LDR + e] = r;
                         rs += r;
                     }
                 }
@@ -231,7 +245,7 @@ uneven_kernel(UnevenParams P)
                 // a_ge = R[g,e] / r_g, w_g = 1 / r_g, phi_g = F_g / r_g (lane per ground state)
                 for (int k = t; k < n_g; k += G) {
                     const double inv = mm_rcp(Rk[k]);  // r_g > 0: every ground state is pumped
-                    for (int e = 0; e < n_e; e++) Rm[k * NEMAX + e] *= inv;
+                    for (int e = 0; e < n_e; e++) Rm[k * LDR + e] *= inv;
                     wg[k] = inv;
                     ph[k] = Fk[k] * inv;
                 }
@@ -240,13 +254,13 @@ uneven_kernel(UnevenParams P)
                 for (int idx = t; idx < n_e * n_e; idx += G) {
                     const int e = idx / n_e, e2 = idx - e * n_e;
                     double a = 0.0;
-                    for (int g = 0; g < n_g; g++) a = fma(Rm[g * NEMAX + e], BR[e2 * n_g + g], a);
+                    for (int g = 0; g < n_g; g++) a = fma(Rm[g * LDR + e], BR[g * NEMAX + e2], a);
                     Kc[e * LDK + e2] = a;
                 }
                 for (int e2 = t; e2 < n_e; e2 += G) {
                     double a = 0.0, b = 0.0, c = 0.0;
                     for (int g = 0; g < n_g; g++) {
-                        const double br = BR[e2 * n_g + g];
+                        const double br = BR[g * NEMAX + e2];
                         a = fma(br, wg[g], a);
                         b = fma(br, ph[g], b);
                         c += br;
@@ -301,7 +315,7 @@ uneven_kernel(UnevenParams P)
                 for (int i = 0; i < n_g; i++) {
                     for (int j = t; j < n_g; j += G) {
                         double a = (i == j) ? -Rk[j] : 0.0;
-                        for (int e = 0; e < n_e; e++) a = fma(Rm[j * NEMAX + e], BR[e * n_g + i], a);
+                        for (int e = 0; e < n_e; e++) a = fma(Rm[j * LDR + e], BR[i * NEMAX + e], a);
                         A[i * LDA + j] = (i == n_g - 1) ? 1.0 : a;
                     }
                 }
