@@ -80,9 +80,8 @@ struct ULayout {
     static constexpr int LDA = NGMAX + 1;
     static constexpr int LDK = NEMAX + 1;
     // row stride of the rates Rm[g][e]: lanes own consecutive ground states,
-    // so an odd stride keeps their row accesses in distinct banks (the
-    // elimination layout keeps NEMAX; its matrix is the larger footprint)
-    static constexpr int LDR = RED ? NEMAX + 1 : NEMAX;
+    // so an odd stride keeps their row accesses in distinct banks
+    static constexpr int LDR = NEMAX + 1;
     // per CTA
     static constexpr int mol_doubles = 2 * (NGMAX + NEMAX) + NGMAX * NEMAX * 3 + NEMAX * NGMAX + NGMAX;
     static constexpr int beam_doubles = 5 * NBU;
@@ -90,7 +89,7 @@ struct ULayout {
     // elimination: A, Rm, bv, xv, invU, Fk, Rk, Esg, fd, Ese
     // reduced:     Rm (scaled rates), K, Fk, Rk, Esg, w, phi, fd, Ese, cw, cf, rs, pi
     static constexpr int grp_raw = RED ? NGMAX * LDR + NEMAX * LDK + 5 * NGMAX + NBU + 5 * NEMAX
-                                       : NGMAX * LDA + NGMAX * NEMAX + 6 * NGMAX + NBU + NEMAX;
+                                       : NGMAX * LDA + NGMAX * LDR + 6 * NGMAX + NBU + NEMAX;
     // two 16-lane groups of a warp read the same offsets of their own region:
     // a stride of 16 banks past a multiple of 128 bytes keeps those reads
     // conflict-free (a multiple of 128 bytes would put both in the same banks)
