@@ -29,6 +29,7 @@ from __future__ import annotations
 import argparse
 import json
 import os
+import platform
 import subprocess
 import sys
 import threading
@@ -41,9 +42,9 @@ sys.path.insert(0, ROOT)
 
 METRIC = "16-level steady-state force evals/s and particle-steps/s: plain FP64 vs FP32+refine @1e-6"
 N_SETS, NV, NZ = 4096, 256, 256
-# dram__bytes_read.sum + dram__bytes_write.sum of one force_reduced_kernel launch
-# over the default workload (11.46 MB + 2.22 GB)
-TRAFFIC_PER_LAUNCH = 2.2315e9
+# dram__bytes_read.sum + dram__bytes_write.sum per point of force_reduced_kernel
+# (FP32 form, grid layout, F only), from an ncu capture of a 512-set launch
+TRAFFIC_PER_POINT = 2.2315e9 / (4096 * 256 * 256)
 SEED = 20261203
 
 
@@ -130,39 +131,138 @@ def hbm_figure(nbytes, ms):
 
 
 def peak_probe(torch):
-    """Measured FP64 and FP32 FMA throughput (TFLOP/s) of this GPU."""
+    """Measured FP64 and FP32 FMA throughput (TFLOP/s) of this GPU, from the
+    FMA-chain probe in molmot_b200/lib/libmolmot_probe.so (a measurement aid
+    built beside the product library, not part of its ABI)."""
     import ctypes
-    from molmot_b200 import _lib
-    L = _lib.load()
+    path = os.path.join(ROOT, "molmot_b200", "lib", "libmolmot_probe.so")
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} is missing; build it with make -C molmot_b200/csrc")
+    L = ctypes.CDLL(path)
+    L.fma_peak_probe.restype = ctypes.c_int
+    L.fma_peak_probe.argtypes = [ctypes.c_int32, ctypes.c_int64, ctypes.POINTER(ctypes.c_double),
+                                 ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]
     out = {}
     for which, name, iters in [(0, "fp64", 4096), (1, "fp32", 16384)]:
         best = 0.0
         for _ in range(3):
             ms, fl = ctypes.c_double(), ctypes.c_double()
-            _lib.check(L.mm_peak_probe(which, iters, ctypes.byref(ms), ctypes.byref(fl),
-                                       ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)),
-                       "mm_peak_probe")
+            rc = L.fma_peak_probe(which, iters, ctypes.byref(ms), ctypes.byref(fl),
+                                  ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+            if rc != 0:
+                raise RuntimeError(f"fma_peak_probe failed (rc={rc})")
             best = max(best, fl.value / (ms.value * 1e-3) / 1e12)
         out[name] = best
     return out
 
 
-def cpu_baseline(mol, n_sets_sample=2048):
-    """The reference's numba core (restated) on all host cores, on a sample of
-    2048 of the 4096 parameter sets (1.3e8 points, about 15 s on 16 cores)."""
-    from oracle import rate_eq_numba as nb
+REF_DIR = os.path.join(ROOT, "baseline", "_ref")
+
+
+def cpu_model():
+    """The host CPU's model name (/proc/cpuinfo)."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return platform.processor() or "unknown"
+
+
+class CpuForceMaps:
+    """CPU force maps of the batched-map workload for the CPU legs.
+
+    kind "reference": the reference's numba core, molmot/obe/rate_equations_jit.py
+    :18-145 (_rate_eq_core), imported unchanged from the reference installed in
+    baseline/_ref, driven by a numba prange harness over the points of each
+    set's (v, z) grid on every host core (numba's default thread count).
+    kind "port": when baseline/_ref is absent, the C restatement of the same
+    core (oracle/rate_eq_oracle.c) with one pthread per host core."""
+
+    def __init__(self, mol):
+        self.mol = mol
+        self.E = np.ascontiguousarray(mol.energies, dtype=np.float64)
+        self.d2 = np.ascontiguousarray(mol.d_squared, dtype=np.float64)
+        self.zd = np.ascontiguousarray(mol.zeeman_z_diag, dtype=np.float64)
+        if os.path.isdir(os.path.join(REF_DIR, "molmot")):
+            os.environ.setdefault("NUMBA_CACHE_DIR", os.path.join(REF_DIR, ".numba_cache"))
+            if REF_DIR not in sys.path:
+                sys.path.insert(0, REF_DIR)
+            import numba
+            from numba import njit, prange
+            from molmot.obe.rate_equations_jit import _rate_eq_core
+
+            @njit(parallel=True)
+            def grid(E, d2, zd, kdir, freq, pol, s0, B, v, z, Gamma, k, geff, n_g, n_e, out):
+                nv, nz = v.shape[0], z.shape[0]
+                per = nv * nz
+                for i in prange(kdir.shape[0] * per):
+                    s = i // per
+                    r = i - s * per
+                    iv = r // nz
+                    out[i] = _rate_eq_core(E, d2, zd, kdir[s], freq[s], pol[s], s0[s], v[iv],
+                                           z[r - iv * nz], B[s], Gamma, k, geff, n_g, n_e)[0]
+
+            self.numba, self.grid, self.kind = numba, grid, "reference"
+            self.what = ("the reference's _rate_eq_core (molmot/obe/rate_equations_jit.py:18-145), "
+                         "unchanged from baseline/_ref, numba prange harness over points")
+        else:
+            from oracle import rate_eq as orc
+            self.orc, self.kind = orc, "port"
+            self.what = ("C restatement of _rate_eq_core (oracle/rate_eq_oracle.c), pthreads over "
+                         "points (the reference install baseline/_ref is absent)")
+
+    def threads(self):
+        return self.numba.get_num_threads() if self.kind == "reference" else self.orc.max_threads()
+
+    def set_threads(self, n):
+        if self.kind == "reference":
+            self.numba.set_num_threads(n)
+        self._n = n
+
+    def __call__(self, kdir, freq, pol, s0, B, v, z):
+        """F [n_sets * nv * nz] of the grids; the reference wrapper's layout:
+        polarisations as float64 (rate_equations_jit.py:155-159)."""
+        m = self.mol
+        if self.kind == "reference":
+            out = np.empty(kdir.shape[0] * v.size * z.size)
+            self.grid(self.E, self.d2, self.zd, np.ascontiguousarray(kdir, dtype=np.float64),
+                      np.ascontiguousarray(freq, dtype=np.float64),
+                      np.ascontiguousarray(pol, dtype=np.float64),
+                      np.ascontiguousarray(s0, dtype=np.float64), np.ascontiguousarray(B, dtype=np.float64),
+                      np.ascontiguousarray(v, dtype=np.float64), np.ascontiguousarray(z, dtype=np.float64),
+                      float(m.Gamma), float(m.k), 1.0, int(m.n_ground), int(m.n_excited), out)
+            return out
+        return self.orc.force_batch(m, kdir, freq, pol, s0, B, v, z, grid=True, want_pop=False,
+                                    n_threads=getattr(self, "_n", 0))[0]
+
+
+def cpu_baseline(mol, n_sets_sample=1024):
+    """The CPU leg of the force maps on the bench host: all cores on 1024 of the
+    4096 parameter sets (6.7e7 points, about 10-20 s), and one thread on 8 sets."""
+    cpu = CpuForceMaps(mol)
     kdir, freq, pol, s0, B = make_params(mol, n_sets_sample, SEED)
     v = np.linspace(-10, 10, NV)
     z = np.linspace(-1e-2, 1e-2, NZ)
-    nb.force_grid(mol, kdir[:1], freq[:1], pol[:1], s0[:1], B[:1], v[:4], z[:4])  # compile
+    cpu(kdir[:1], freq[:1], pol[:1], s0[:1], B[:1], v[:4], z[:4])  # compile
+    threads = cpu.threads()
     t0 = time.perf_counter()
-    nb.force_grid(mol, kdir, freq, pol, s0, B, v, z)
+    cpu(kdir, freq, pol, s0, B, v, z)
     dt = time.perf_counter() - t0
     n = n_sets_sample * NV * NZ
-    return {"value": n / dt, "unit": "force evals/s", "cores": nb.threads(), "kind": "port",
-            "sample": f"{n_sets_sample} of the {N_SETS} parameter sets, full {NV}x{NZ} grid "
-                      f"({n} points, {dt:.2f} s), numba restatement of _rate_eq_core, "
-                      f"prange over points, os.cpu_count()={os.cpu_count()}"}
+    one = 8
+    cpu.set_threads(1)
+    t1 = time.perf_counter()
+    cpu(kdir[:one], freq[:one], pol[:one], s0[:one], B[:one], v, z)
+    dt1 = time.perf_counter() - t1
+    cpu.set_threads(threads)
+    return {"value": n / dt, "unit": "force evals/s", "cores": threads, "kind": cpu.kind,
+            "sample": f"{n_sets_sample} of the {N_SETS} parameter sets x full {NV}x{NZ} grid "
+                      f"({n} points, {dt:.2f} s): {cpu.what}",
+            "one_thread": {"value": one * NV * NZ / dt1, "sample": f"{one} sets x {NV}x{NZ} grid"},
+            "cpu_model": cpu_model(), "os_cpu_count": os.cpu_count()}
 
 
 def _ev_time(torch, fn, reps=3):
@@ -177,7 +277,7 @@ def _ev_time(torch, fn, reps=3):
     return e0.elapsed_time(e1) / reps
 
 
-def secondary_measurements(torch, mol, pack, dev):
+def secondary_measurements(torch, mol, pack, dev, peaks):
     """Particle-steps/s of the trajectory ensembles and the adjoint's cost."""
     from molmot_b200.engine import BeamSets, force_batch, force_adjoint, traj
     from molmot_b200.fields import make_dc_mot_beams
@@ -194,8 +294,19 @@ def secondary_measurements(torch, mol, pack, dev):
     ps = N3 * S3 / (ms * 1e-3)
     out["traj3d"] = {"metric": "particle-steps/s", "value": ps, "particles": N3, "steps": S3,
                      "ms": ms, "workload": "SrOH 3D quadrupole MOT, 24 beams, leapfrog dt=1us, "
-                     "Philox recoil kicks, FP64 state; full 65,536 x 30,000-step run "
-                     f"extrapolates to {N3 * 30000 / ps:.0f} s"}
+                     "Philox recoil kicks, FP64 state"}
+    # a 1000-step chunk of the same ensemble (one launch, timed once)
+    from molmot_b200.constants import hbar as HBAR_CODATA
+    from molmot_b200.engine import pack_for, traj3d
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    o3 = traj3d(pack_for(mol), sim3._bs(), r0, v0, 1e-6, 1000, kicks=True, seed=SEED, hbar=HBAR_CODATA)
+    e1.record()
+    torch.cuda.synchronize()
+    ms_l = e0.elapsed_time(e1)
+    out["traj3d"]["long"] = {"steps": 1000, "ms": ms_l, "value": N3 * 1000 / (ms_l * 1e-3),
+                             "alive_fraction": float((o3["r"].norm(dim=1) <= 0.015).double().mean())}
     # 1D DC MOT ensemble (the reference's trajectory configuration), 65,536 particles
     bs1 = BeamSets.from_beams(make_dc_mot_beams(mol, -0.20, 0.70, 1.0), 0.16)
     z0 = torch.as_tensor(rng.normal(0, 2e-3, 65536), device=dev)
@@ -252,23 +363,27 @@ def secondary_measurements(torch, mol, pack, dev):
                       "forward_ms": tf, "forward_plus_adjoint_ms": ta, "cost_ratio": ta / tf,
                       "reduced": {"forward_ms": trf, "forward_plus_adjoint_ms": tra,
                                   "cost_ratio": tra / trf, "vs_elimination_adjoint": ta / tra}}
-    out["uneven"] = uneven_measurement(torch, dev)
+    out["uneven"] = uneven_measurement(torch, dev, peaks)
     return out
 
 
-def uneven_measurement(torch, dev):
+def uneven_measurement(torch, dev, peaks):
     """The uneven batch: 2048 synthetic molecules (n_ground 4..48, n_excited
     4..16), 64..4096 points each, in one persistent launch per size class
     (warps per CTA from the autotuner), its CUDA-graph replay, and one launch
-    per molecule on every 8th molecule, scaled to the whole batch by points."""
+    per molecule on every 8th molecule, scaled to the whole batch by points.
+    Roofline: the batch's algorithmic FP64 FLOP (flops.uneven_flops) over the
+    persistent time, against the FP64 FMA peak."""
     from molmot_b200.engine import BeamSets
-    from molmot_b200.uneven import MoleculeBank, UnevenBatch, make_uneven_workload
+    from molmot_b200.flops import uneven_flops
+    from molmot_b200.uneven import MoleculeBank, UnevenBatch, make_uneven_workload, sample_molecules
     mols, counts, (kd, fr, po, s0), Bu, vu, zu = make_uneven_workload(n_mol=2048, seed=SEED)
     ub = UnevenBatch(MoleculeBank(mols), counts, BeamSets(kd, fr, po, s0, Bu))
     vd = torch.as_tensor(vu, device=dev)
     zd = torch.as_tensor(zu, device=dev)
     wpc = ub.autotune(vd, zd)
     ms_p = _ev_time(torch, lambda: ub.force(vd, zd), 3)
+    F = ub.force(vd, zd)["F"].cpu().numpy()
     g, _, _, _ = ub.graph(vd, zd)
     ms_g = _ev_time(torch, g.replay, 3)
     del g
@@ -283,15 +398,68 @@ def uneven_measurement(torch, dev):
     ms_s = _ev_time(torch, lambda: [u.force(a, b) for u, a, b in singles], 2)
     pts_s = int(sum(counts[i] for i in sample))
     n = int(off[-1])
+    fl = uneven_flops(mols, counts, po)
+    achieved = fl / (ms_p * 1e-3) / 1e12
+    pick = sample_molecules([m.n_ground for m in mols], [m.n_excited for m in mols], counts)
+    check = [(mols[m], (kd[m:m + 1], fr[m:m + 1], po[m:m + 1], s0[m:m + 1], Bu[m:m + 1]),
+              vu[off[m]:off[m + 1]], zu[off[m]:off[m + 1]], F[off[m]:off[m + 1]]) for m in pick]
     return {"metric": "force evals/s", "points": n, "molecules": len(mols),
             "persistent_ms": ms_p, "persistent_value": n / (ms_p * 1e-3),
             "graph_replay_ms": ms_g, "warps_per_cta": list(wpc),
             "per_molecule_launches_ms_estimate": ms_s * n / pts_s,
             "per_molecule_sample": f"{len(sample)} molecules ({pts_s} points), scaled by points",
+            "roofline": {"bound": "fp64", "achieved": achieved, "peak": peaks["fp64"],
+                         "unit": "TFLOP/s", "frac": achieved / peaks["fp64"],
+                         "flops_per_point_mean": fl / n},
             "workload": "2048 synthetic molecules, n_ground 4..48, n_excited 4..16, 64..4096 "
                         "(v, z) points each; FP64 rates in the reference's order, populations "
                         "from the FP64 excited-chain solve (the reference's elimination for "
-                        "molecules the reduction does not cover)"}
+                        "molecules the reduction does not cover)",
+            "_check": check}
+
+
+def uneven_oracle_check(check):
+    """The uneven batch's forces against the CPU oracle on the sample of
+    sample_molecules (4 molecules per size class, including the most points
+    and n_ground 48): max |dF| / max |F| per molecule (the checker; part of
+    the cpu_baseline leg)."""
+    from oracle import rate_eq as orc
+    worst = 0.0
+    for mol, (kd, fr, po, s0, B), v, z, F in check:
+        Fo = orc.force_batch(mol, kd, fr, po, s0, B, v, z, want_pop=False)[0]
+        worst = max(worst, float(np.abs(F - Fo).max() / np.abs(Fo).max()))
+    return {"max": worst, "molecules": len(check),
+            "points": int(sum(len(c[2]) for c in check)),
+            "n_ground": sorted({int(c[0].n_ground) for c in check})}
+
+
+def evidence_line(plain, red64, accuracy, secondary):
+    """The measured figures beside the headline, compact (numbers only)."""
+    r = lambda x, d=4: float(f"{x:.{d}g}") if x is not None else None
+    ev = {"plain_fp64": {"value": r(plain["value"]), "ms": r(plain["ms_per_step"]),
+                         "frac_fp64": r(plain["roofline"]["frac"], 3),
+                         "fp32_form_speedup": r(plain["fp32_form_speedup"], 3)},
+          "fp64_reduced": {"value": r(red64["value"]), "ms": r(red64["ms_per_step"]),
+                           "diff_vs_plain": r(red64["max_rel_diff_vs_plain_fp64_per_set"], 2)},
+          "acc_fp32_vs_fp64": {k: r(accuracy["fp32_vs_fp64_per_set"][k], 2) for k in ("max", "p99")}}
+    if "vs_oracle" in accuracy:
+        ev["acc_vs_oracle"] = {k: r(v["max"], 2) for k, v in accuracy["vs_oracle"].items()}
+    if secondary:
+        t3, u = secondary["traj3d"], secondary["uneven"]
+        ev["traj3d"] = {"value": r(t3["value"]), "ms": r(t3["ms"]), "steps": t3["steps"]}
+        if "long" in t3:
+            ev["traj3d"]["long"] = {k: r(v) for k, v in t3["long"].items()}
+        ev["traj1d"] = {"fp64": r(secondary["traj1d"]["value"]), "fp32": r(secondary["traj1d_fp32"]["value"])}
+        ev["traj_grad"] = {"value": r(secondary["traj_grad"]["value"]),
+                           "vs_forward": r(secondary["traj_grad"]["cost_ratio_vs_fp64_forward"], 3)}
+        ev["adjoint_cost"] = {"fp64": r(secondary["adjoint"]["cost_ratio"], 3),
+                              "reduced": r(secondary["adjoint"]["reduced"]["cost_ratio"], 3)}
+        ev["uneven"] = {"value": r(u["persistent_value"]), "ms": r(u["persistent_ms"]),
+                        "frac_fp64": r(u["roofline"]["frac"], 3), "graph_ms": r(u["graph_replay_ms"]),
+                        "per_molecule_ms": r(u["per_molecule_launches_ms_estimate"])}
+        if "accuracy_vs_oracle" in u:
+            ev["uneven"]["acc_vs_oracle"] = r(u["accuracy_vs_oracle"]["max"], 2)
+    return ev
 
 
 def oracle_check(mol, pack, bs, v_d, z_d, kdir, freq, pol, s0, B, sets=(0, 1, 2047, 4095)):
@@ -317,28 +485,32 @@ def oracle_check(mol, pack, bs, v_d, z_d, kdir, freq, pol, s0, B, sets=(0, 1, 20
 
 
 def run_reference_arm(args):
+    """The reference's own CPU path of the force maps (CpuForceMaps: its
+    numba core from baseline/_ref on every host core), on this workload's
+    metric and unit.  Each step is a bounded sample: 32 of the 4096 parameter
+    sets over the full 256 x 256 grid.  Rank 0 only."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     from molmot_b200.molecules import load_sroh_from_julia
-    from oracle import rate_eq_numba as nb
     mol = load_sroh_from_julia()
-    n_sample = 64  # 4.2e6 points per step, under a second on 16 cores
+    cpu = CpuForceMaps(mol)
+    n_sample = 32
     kdir, freq, pol, s0, B = make_params(mol, n_sample, SEED)
     v = np.linspace(-10, 10, NV)
     z = np.linspace(-1e-2, 1e-2, NZ)
-    nb.force_grid(mol, kdir[:1], freq[:1], pol[:1], s0[:1], B[:1], v[:4], z[:4])
+    cpu(kdir[:1], freq[:1], pol[:1], s0[:1], B[:1], v[:4], z[:4])  # compile
     for _ in range(args.warmup):
-        nb.force_grid(mol, kdir, freq, pol, s0, B, v, z)
+        cpu(kdir, freq, pol, s0, B, v, z)
     times = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        nb.force_grid(mol, kdir, freq, pol, s0, B, v, z)
+        cpu(kdir, freq, pol, s0, B, v, z)
         times.append(time.perf_counter() - t0)
     n = n_sample * NV * NZ
     val = n / (sum(times) / len(times))
     sample = (f"each step: {n_sample} of the {N_SETS} parameter sets x full {NV}x{NZ} grid "
-              f"({n} points) on the host CPU")
+              f"({n} points) on the host CPU; {cpu.what}")
     line = {"impl": "reference", "metric": METRIC, "value": val, "unit": "force evals/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True,
@@ -346,8 +518,9 @@ def run_reference_arm(args):
             "config": {"workload": f"SrOH batched force maps, {N_SETS} sets x {NV}x{NZ} (v,z) grid, "
                                    "8-beam DC MOT (bounded CPU sample per step)",
                        "sets_per_step_sample": n_sample},
-            "cpu_baseline": {"value": val, "unit": "force evals/s", "cores": nb.threads(),
-                             "kind": "port", "sample": sample},
+            "cpu_baseline": {"value": val, "unit": "force evals/s", "cores": cpu.threads(),
+                             "kind": cpu.kind, "sample": sample, "cpu_model": cpu_model(),
+                             "os_cpu_count": os.cpu_count()},
             "e2e": {"value": val, "unit": "force evals/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -530,7 +703,7 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     ms_e2e = float(t.item())
 
-    secondary = (secondary_measurements(torch, mol, pack, dev)
+    secondary = (secondary_measurements(torch, mol, pack, dev, peaks)
                  if world == 1 and not args.no_secondary else None)
 
     A = active_triples(mol.d_squared, pol[0])
@@ -546,53 +719,64 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(mol)
         accuracy["vs_oracle"] = oracle_check(mol, pack, bs, v_d, z_d, kdir, freq, pol, s0, B)
+        if secondary is not None:
+            secondary["uneven"]["accuracy_vs_oracle"] = uneven_oracle_check(secondary["uneven"].pop("_check"))
+    elif secondary is not None:
+        secondary["uneven"].pop("_check", None)
 
     if rank == 0:
         total = n_pts * world
+        plain = {"value": total / (ms64 * 1e-3), "unit": "force evals/s", "ms_per_step": ms64,
+                 "fp32_form_speedup": ms64 / ms32,
+                 "roofline": {"bound": "fp64", "achieved": achieved64, "peak": peaks["fp64"],
+                              "unit": "TFLOP/s", "frac": achieved64 / peaks["fp64"]}}
+        red64 = {"value": total / (ms64r * 1e-3), "unit": "force evals/s", "ms_per_step": ms64r,
+                 "max_rel_diff_vs_plain_fp64_per_set": err64r}
+        roof = {"bound": "fp64+fp32", "achieved": achieved32, "peak": peak32, "unit": "TFLOP/s",
+                "frac": achieved32 / peak32,
+                "traffic": TRAFFIC_PER_POINT * n_pts, "traffic_unit": "bytes per launch",
+                "algorithmic_bytes": 8 * n_pts,
+                "peak_source": f"FMA probe on this GPU: fp64 {peaks['fp64']:.1f}, fp32 "
+                               f"{peaks['fp32']:.1f} TFLOP/s",
+                "flops_per_point": {"fp64": f64_32, "fp32": f32_32}}
+        e2e = {"value": total / (ms_e2e * 1e-3), "unit": "force evals/s",
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "ms_per_step": ms_e2e,
+               "api": "engine.force_maps_to_host, 256-set chunks"}
+        details = {"bench_details": {
+            "plain_fp64": plain, "fp64_reduced": red64, "accuracy": accuracy, "secondary": secondary,
+            "roofline": dict(roof, hbm=hbm_figure(8 * n_pts, ms32),
+                             reference_algorithm_equivalent_tflops=f64_64 * n_pts / (ms32 * 1e-3) / 1e12,
+                             traffic_source="DRAM read + write per point of an ncu capture of "
+                                            "force_reduced_kernel (512 sets), times the points"),
+            "cpu_baseline": cpu, "e2e": e2e, "clocks": clk}}
+        # everything, first (long); then the compact evidence line and the
+        # headline, which are the last lines of the output
+        print(json.dumps(details), flush=True)
+        print(json.dumps({"evidence": evidence_line(plain, red64, accuracy, secondary)}), flush=True)
         line = {
             "metric": METRIC, "value": total / (ms32 * 1e-3), "unit": "force evals/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms32,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
             "data": "synthetic",
-            "config": {"workload": f"SrOH (12 ground + 4 excited) batched force maps: {n_sets} "
-                                   f"parameter sets x {NV}x{NZ} (v, z) grid per GPU, 8-beam DC MOT, "
-                                   "FP32 Lorentzians, FP64 sums, FP64 excited-chain population solve",
+            "config": {"workload": f"SrOH 12+4 levels, {n_sets} parameter sets x {NV}x{NZ} (v, z) "
+                                   "grid per GPU, 8-beam DC MOT; FP32 Lorentzians, FP64 sums and "
+                                   "excited-chain solve",
                        "points_per_step_per_gpu": n_pts, "parallelism": f"sets sharded, {world} GPU(s)",
-                       "l2": "256 MB buffer written between timed steps (> 126 MB L2)"},
-            "plain_fp64": {"value": total / (ms64 * 1e-3), "unit": "force evals/s",
-                           "ms_per_step": ms64, "ratio_fp32_over_fp64": ms64 / ms32,
-                           "roofline": {"bound": "fp64", "achieved": achieved64,
-                                        "peak": peaks["fp64"], "unit": "TFLOP/s",
-                                        "frac": achieved64 / peaks["fp64"]}},
-            "fp64_reduced": {"value": total / (ms64r * 1e-3), "unit": "force evals/s",
-                             "ms_per_step": ms64r,
-                             "max_rel_diff_vs_plain_fp64_per_set": err64r,
-                             "form": "FP64 rates in the plain form's order, populations from the "
-                                     "FP64 excited-chain solve"},
-            "roofline": {"bound": "fp64+fp32", "achieved": achieved32, "peak": peak32,
-                         "unit": "TFLOP/s", "frac": achieved32 / peak32,
-                         # DRAM read + write of one full launch, ncu capture in
-                         # profiles/force_reduced_kernel_sroh_maps.md (4096 sets)
-                         "traffic": TRAFFIC_PER_LAUNCH if n_sets == N_SETS else None,
-                         "traffic_unit": "bytes per launch",
-                         "algorithmic_bytes": 8 * n_pts,
-                         "hbm": hbm_figure(8 * n_pts, ms32),
-                         "peak_source": "mm_peak_probe FMA loop on this GPU: "
-                                        f"fp64 {peaks['fp64']:.2f}, fp32 {peaks['fp32']:.2f} TFLOP/s",
-                         "flops_per_point": {"fp64": f64_32, "fp32": f32_32},
-                         "reference_algorithm_equivalent_tflops": f64_64 * n_pts / (ms32 * 1e-3) / 1e12},
-            "e2e": {"value": total / (ms_e2e * 1e-3), "unit": "force evals/s",
-                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-                    "ms_per_step": ms_e2e,
-                    "api": "molmot_b200.engine.force_maps_to_host (256-set chunks, copies "
-                           "overlapped with computation)"},
-            "accuracy": accuracy,
-            "secondary": secondary,
+                       "l2": "256 MB written between timed steps"},
+            "roofline": {k: roof[k] for k in ("bound", "achieved", "peak", "unit", "frac", "traffic",
+                                              "peak_source")},
+            "e2e": e2e,
             "gpu_launches": args.steps * 3,
-            "clocks": clk,
+            "clocks": {k: clk.get(k) for k in ("sm_mhz", "sm_max_mhz", "reasons")},
         }
         if cpu is not None:
-            line["cpu_baseline"] = cpu
+            line["cpu_baseline"] = {"value": cpu["value"], "unit": cpu["unit"], "cores": cpu["cores"],
+                                    "kind": cpu["kind"],
+                                    "sample": f"1024 of 4096 sets x 256x256 grid; {cpu['kind']}: "
+                                              + ("the reference's _rate_eq_core unchanged, numba prange"
+                                                 if cpu["kind"] == "reference" else "C restatement"),
+                                    "one_thread": round(cpu["one_thread"]["value"]),
+                                    "cpu_model": cpu["cpu_model"]}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()

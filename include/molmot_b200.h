@@ -199,10 +199,13 @@ MM_API int mm_uneven_force(const mm_uneven_plan *plan, const mm_beams *beams, co
  * library's device memory (per GPU), so a batch may make at most 43,680 work
  * items (point chunks of chunk_groups CTA widths); a larger one is refused
  * with an error naming the limit.  The counters are zeroed on `stream` by
- * every call.  The first call on each GPU looks up the array's device
- * address (cudaGetSymbolAddress); it must come before any stream capture on
- * that GPU.  Calls share the array and host staging arrays: calls that
- * overlap in time (two host threads, or two streams of one GPU) race.
+ * every call.  The first call on each GPU (and the first after a reset of
+ * its context) looks up the array's device address (cudaGetSymbolAddress);
+ * make that first call before any stream capture on that GPU.  Calls share
+ * the array and host staging arrays: two calls race unless the second is
+ * ordered after the first on the GPU -- issued on the same stream, or on a
+ * stream that waits on an event recorded after the first call -- and calls
+ * from two host threads at once race on the host arrays.
  */
 MM_API int mm_uneven_force_static(const mm_bank *bank, const mm_beams *beams,
                                   const int64_t *point_offsets, const mm_uneven_opts *opts,
@@ -323,13 +326,6 @@ MM_API int mm_traj3d_run(const mm_pack *pack, const mm_beams *beams, const doubl
                          void *stream);
 
 /*
- * FMA-throughput probe (measurement aid; no counterpart in the reference).
- * which = 0: FP64, 1: FP32.  Runs a register-only FMA loop on every SM and
- * writes its duration (ms) and FLOP count (2 per FMA); synchronises `stream`.
- * Used as the roofline peak of the force kernels, which are bound by the
- * FP64/FP32 CUDA-core pipes.
- */
-/*
  * Per-time-bin statistics of a trajectory ensemble (the reductions of
  * sigma_vs_time, temperature_vs_time and density_vs_time,
  * molmot/mot/analysis.py:128-287).  z, v: device arrays, value of particle p
@@ -350,9 +346,6 @@ MM_API int mm_ensemble_stats(const double *z, const double *v, int64_t n_particl
  */
 MM_API int mm_histogram(const double *x, int64_t n, int64_t stride, double lo, double hi, int32_t bins,
                         uint64_t *counts, void *stream);
-
-MM_API int mm_peak_probe(int32_t which, int64_t iters, double *ms_out, double *flops_out,
-                         void *stream);
 
 #ifdef __cplusplus
 }

@@ -111,7 +111,6 @@ SIGNATURES = {
                                          ctypes.c_double, _vp, _vp]),
     "mm_histogram": (ctypes.c_int, [_vp, ctypes.c_int64, ctypes.c_int64, ctypes.c_double, ctypes.c_double,
                                     ctypes.c_int32, _vp, _vp]),
-    "mm_peak_probe": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int64, _dp, _dp, _vp]),
     "mm_traj_grad_run": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(TgradOpts), ctypes.c_int64, _vp, _vp,
                                         _vp, _vp]),
 }

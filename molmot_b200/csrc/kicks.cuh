@@ -24,8 +24,9 @@ __device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k)
 
 __device__ __forceinline__ double u01(unsigned x) { return ((double)x + 0.5) * 2.3283064365386963e-10; }
 
-// Recoil kick of one step (the oracle's recoil_kick): N ~ Poisson(lam) by
-// sequential inversion, then 2N isotropic unit vectors times v_rec.
+// Recoil kick of one step: N ~ Poisson(lam) events by sequential inversion
+// of one uniform draw, then 2N isotropic unit vectors (absorption and
+// emission) times v_rec, from the Philox counters (particle, step, draw, 0).
 __device__ int recoil_kick(unsigned long long seed, unsigned particle, unsigned step, double lam,
                            double v_rec, double kick[3])
 {

@@ -678,8 +678,10 @@ extern "C" int mm_uneven_force(const mm_uneven_plan *plan, const mm_beams *beams
 // process exits); the host side stages the work list in fixed host arrays.
 // Capacity: MM_STATIC_SCRATCH_BYTES = 1 MiB, i.e. kStaticMaxTasks = 43,680
 // work items (each covers chunk_groups x groups-per-CTA points).
-// Calls share that array and the host arrays: calls that overlap, from two
-// host threads or on two streams of one GPU, race.
+// Calls share that array and the host arrays.  Two calls race unless the
+// second is ordered after the first on the GPU (the same stream, or a wait
+// on an event recorded after the first call), and calls from two host
+// threads race on the host arrays.
 #define MM_STATIC_SCRATCH_BYTES (1u << 20)
 static __device__ __align__(256) unsigned char g_uneven_scratch[MM_STATIC_SCRATCH_BYTES];
 
@@ -691,7 +693,46 @@ UnevenTask h_st_tasks[kStaticMaxTasks];   // in creation order
 UnevenTask h_st_sorted[kStaticMaxTasks];  // in launch order
 double h_st_cost[kStaticMaxTasks];
 int h_st_order[kStaticMaxTasks];
-void *g_scratch_dev[kMaxDevices];         // address of g_uneven_scratch per device ordinal
+// Device address of g_uneven_scratch per device ordinal, with the id of the
+// context it was looked up in: after cudaDeviceReset the module is loaded
+// again in a new context, possibly at another address, so the address is
+// looked up again whenever the current context is a different one.
+struct ScratchAddr {
+    unsigned long long ctx_id;
+    void *ptr;
+};
+ScratchAddr g_scratch_dev[kMaxDevices];
+
+// Id of the calling thread's current CUDA context (driver entry points
+// cuCtxGetCurrent / cuCtxGetId, resolved through the runtime so the library
+// does not link libcuda); 0 when no context is current.
+int current_context_id(unsigned long long *id)
+{
+    typedef int (*GetCurrent)(void **);
+    typedef int (*GetId)(void *, unsigned long long *);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    if (!get_current || !get_id) {
+        void *a = nullptr, *b = nullptr;
+        cudaDriverEntryPointQueryResult qa, qb;
+        if (mm_cuda_check(cudaGetDriverEntryPoint("cuCtxGetCurrent", &a, cudaEnableDefault, &qa),
+                          "cudaGetDriverEntryPoint(cuCtxGetCurrent)") ||
+            mm_cuda_check(cudaGetDriverEntryPoint("cuCtxGetId", &b, cudaEnableDefault, &qb),
+                          "cudaGetDriverEntryPoint(cuCtxGetId)"))
+            return -3;
+        if (qa != cudaDriverEntryPointSuccess || qb != cudaDriverEntryPointSuccess || !a || !b) {
+            mm_set_error("the driver does not provide cuCtxGetCurrent / cuCtxGetId");
+            return -3;
+        }
+        get_current = (GetCurrent)a;
+        get_id = (GetId)b;
+    }
+    void *ctx = nullptr;
+    if (get_current(&ctx) != 0) { mm_set_error("cuCtxGetCurrent failed"); return -3; }
+    *id = 0;
+    if (ctx && get_id(ctx, id) != 0) { mm_set_error("cuCtxGetId failed"); return -3; }
+    return 0;
+}
 }  // namespace
 
 extern "C" int mm_uneven_force_static(const mm_bank *bank, const mm_beams *beams,
@@ -715,10 +756,17 @@ extern "C" int mm_uneven_force_static(const mm_bank *bank, const mm_beams *beams
     int dev = 0;
     if (mm_cuda_check(cudaGetDevice(&dev), "cudaGetDevice")) return -3;
     if (dev < 0 || dev >= kMaxDevices) { mm_set_error("device ordinal %d is above %d", dev, kMaxDevices - 1); return -1; }
-    if (!g_scratch_dev[dev]) {  // first call on this device
+    // set-up: the array's device address, looked up on the first call on this
+    // device and again after a context reset (the host name of the array is
+    // not a device address)
+    unsigned long long ctx = 0;
+    if (current_context_id(&ctx)) return -3;
+    if (!g_scratch_dev[dev].ptr || ctx == 0 || ctx != g_scratch_dev[dev].ctx_id) {
         void *p = nullptr;
         if (mm_cuda_check(cudaGetSymbolAddress(&p, g_uneven_scratch), "cudaGetSymbolAddress")) return -3;
-        g_scratch_dev[dev] = p;
+        if (current_context_id(&ctx)) return -3;  // the lookup makes the primary context current
+        g_scratch_dev[dev].ptr = p;
+        g_scratch_dev[dev].ctx_id = ctx;
     }
     mm_uneven_plan plan;  // a view of the fixed array; owns no memory
     plan.bank = bank;
@@ -771,7 +819,7 @@ extern "C" int mm_uneven_force_static(const mm_bank *bank, const mm_beams *beams
         plan.n_tasks[c] = n;
         base += n;
     }
-    unsigned char *scr = (unsigned char *)g_scratch_dev[dev];
+    unsigned char *scr = (unsigned char *)g_scratch_dev[dev].ptr;
     UnevenTask *d_tasks = (UnevenTask *)(scr + kScratchHead);
     for (int c = 0, b = 0; c < 3; b += plan.n_tasks[c], c++) plan.d_tasks[c] = d_tasks + b;
     plan.d_counter = (int *)scr;

@@ -51,3 +51,45 @@ def flops_reduced(n_g: int, n_e: int, A: int):
     final = 3 * 2 * n_e + 3
     fp64 = 3 * A + n_g * per_g + gth + final
     return float(fp64), float(fp32)
+
+
+def flops_reduced64(n_g: int, n_e: int, A: int) -> float:
+    """FP64 FLOP of one point of the FP64-reduced form (the uneven batch's
+    form for molecules the reduction covers): the plain form's rates
+    (18 FLOP per active triple) and the excited-chain solve of
+    flops_reduced."""
+    fp64, _ = flops_reduced(n_g, n_e, A)
+    return float(fp64 - 3 * A + 18 * A)
+
+
+def reduction_covers(d_squared, pols) -> bool:
+    """Host twin of the reduced form's structural check for one parameter
+    set: every ground state has an active triple, and the excited-state chain
+    (e' -> e when e' decays to a ground state that a beam excites to e) is
+    strongly connected."""
+    d2 = np.asarray(d_squared)
+    n_g, n_e, _ = d2.shape
+    act = np.zeros((n_g, n_e), dtype=bool)
+    for q in np.asarray(pols).ravel():
+        act |= d2[:, :, int(q)] >= 1e-15
+    if not act.any(axis=1).all():
+        return False
+    decays = d2.sum(axis=2).T > 0  # [e, g]: e decays to g
+    reach = np.eye(n_e, dtype=bool) | (decays.astype(int) @ act.astype(int) > 0)
+    for k in range(n_e):
+        reach |= reach[:, [k]] & reach[[k], :]
+    return bool(reach.all())
+
+
+def uneven_flops(mols, counts, pols) -> float:
+    """Algorithmic FP64 FLOP of an uneven batch: per molecule its points times
+    the FP64-reduced count, or the plain count where the reduction does not
+    cover it (the elimination then runs)."""
+    total = 0.0
+    for m, c, p in zip(mols, counts, pols):
+        A = active_triples(m.d_squared, p)
+        if reduction_covers(m.d_squared, p):
+            total += c * flops_reduced64(m.n_ground, m.n_excited, A)
+        else:
+            total += c * flops_per_point(m.n_ground, m.n_excited, len(np.asarray(p).ravel()), A)[0]
+    return total

@@ -111,10 +111,17 @@ class UnevenBatch:
     def force_static(self, v, z, out, stream=None, uniform_fallback=False):
         """The same forces through mm_uneven_force_static, which allocates
         nothing: the caller passes `out` (F, and optionally R and status) and
-        the work list lives in the library's fixed device array.  Calls that
-        overlap in time race on that array."""
+        the work list lives in the library's fixed device array.  Two calls
+        race on that array unless the second is ordered after the first on
+        the GPU (the same stream, or a wait on an event recorded after the
+        first).  v and z that are not float64, contiguous and on the current
+        CUDA device are converted (a copy, which allocates); `out` must
+        already be in that form."""
+        v = _to_dev(v)
+        z = _to_dev(z)
         if v.numel() != self.n_points or z.numel() != self.n_points:
             raise ValueError(f"expected {self.n_points} points")
+        check_static_out(out, self.n_points, v.device)
         o = _lib.UnevenOpts()
         for i in range(3):
             o.warps_per_cta[i] = int(self.wpc[i])
@@ -189,6 +196,64 @@ class UnevenBatch:
             except Exception:
                 pass
             self.plan = None
+
+
+def sample_molecules(n_ground, n_excited, counts, per_class: int = 4, seed: int = 0):
+    """Indices of a parity sample of an uneven batch: per size class
+    (n_ground <= 16, <= 32, <= 48) the molecule with the most points, the
+    one with the most ground states, the one with the most excited states,
+    and random others of the class up to ``per_class`` (fewer if the class
+    is smaller), in ascending order."""
+    ng = np.asarray(n_ground)
+    ne = np.asarray(n_excited)
+    cnt = np.asarray(counts)
+    cls = np.where(ng <= 16, 0, np.where(ng <= 32, 1, 2))
+    rng = np.random.default_rng(seed)
+    picked = []
+    for c in range(3):
+        idx = np.flatnonzero(cls == c)
+        if idx.size == 0:
+            continue
+        chosen = []
+        for key in (cnt, ng, ne):
+            i = int(idx[np.argmax(key[idx])])
+            if i not in chosen:
+                chosen.append(i)
+        rest = [int(i) for i in rng.permutation(idx) if int(i) not in chosen]
+        chosen += rest[:max(0, per_class - len(chosen))]
+        picked += chosen[:max(per_class, 3)]
+    return sorted(picked)
+
+
+_STATIC_OUT = {"F": torch.float64, "R": torch.float64, "status": torch.int32}
+
+
+def check_static_out(out, n_points: int, device: torch.device) -> None:
+    """Checks the caller's output buffers of ``UnevenBatch.force_static``
+    before their addresses go to the kernels: F is required, R and status
+    optional; each must have its dtype (float64, float64, int32), be
+    contiguous, hold n_points elements and live on ``device``.  Raises
+    ValueError otherwise (a host tensor or a short buffer would make the
+    kernels write outside it)."""
+    if not isinstance(out, dict) or out.get("F") is None:
+        raise ValueError("out must be a dict holding at least the 'F' tensor")
+    for key in out:
+        if key not in _STATIC_OUT:
+            raise ValueError(f"unknown output {key!r}; expected F, R or status")
+    for key, dtype in _STATIC_OUT.items():
+        t = out.get(key)
+        if t is None:
+            continue
+        if not isinstance(t, torch.Tensor):
+            raise ValueError(f"out[{key!r}] must be a torch tensor")
+        if t.dtype != dtype:
+            raise ValueError(f"out[{key!r}] must be {dtype}, got {t.dtype}")
+        if t.device != device:
+            raise ValueError(f"out[{key!r}] must be on {device}, got {t.device}")
+        if not t.is_contiguous():
+            raise ValueError(f"out[{key!r}] must be contiguous")
+        if t.numel() != n_points:
+            raise ValueError(f"out[{key!r}] must hold {n_points} elements, got {t.numel()}")
 
 
 def make_uneven_workload(n_mol: int = 2048, seed: int = 20261203, min_pts: int = 64,

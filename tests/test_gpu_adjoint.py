@@ -181,3 +181,50 @@ def test_adjoint_rejects_fp32(mol, gpu):
     bs = BeamSets(g["kdir"][:1], g["freq"][:1], g["pol"][:1], g["s0"][:1], g["B"][:1])
     with pytest.raises(ValueError):
         force_adjoint(pack_for(mol), bs, g["v"][:4], g["z"][:4], precision="fp32")
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp64_reduced"])
+def test_mot_coefficient_gradients_at_config_scale(mol, gpu, precision):
+    """Gradients of k and beta (33-point stencils) for 32 of the 1024
+    parameter sets of the differentiation workload (bench.py: every 32nd set
+    of make_params(mol, 1024, SEED + 7)), against FP64 torch autograd of the
+    same coefficients through the dense restatement: 1e-8 of each set's
+    largest gradient component, per coefficient and parameter group."""
+    import bench
+    from molmot_b200.autograd import mot_coefficients, stencil_weights
+    from oracle import torch_dense as td
+    kdir, freq, pol, s0, B = bench.make_params(mol, 1024, bench.SEED + 7)
+    idx = np.arange(0, 1024, 32)
+    kdir, freq, pol, s0, B = kdir[idx], freq[idx], pol[idx], s0[idx], B[idx]
+    ref = freq[:, ::2].copy()  # 4 frequencies (each shared by a +z/-z pair)
+    det0 = np.zeros_like(ref)
+    s00 = s0[:, ::2].copy()
+
+    def leaves(dev):
+        f = torch.tensor(det0, dtype=torch.float64, device=dev, requires_grad=True)
+        p = torch.tensor(s00, dtype=torch.float64, device=dev, requires_grad=True)
+        b = torch.tensor(B, dtype=torch.float64, device=dev, requires_grad=True)
+        fr = (torch.as_tensor(ref, dtype=torch.float64, device=dev) + f).repeat_interleave(2, 1)
+        return f, p, b, fr, p.repeat_interleave(2, 1)
+
+    f1, p1, b1, fr1, s01 = leaves(gpu)
+    k1, be1 = mot_coefficients(mol, kdir, pol, fr1, s01, b1, precision=precision)
+    g1 = [torch.autograd.grad(c.sum(), [f1, p1, b1], retain_graph=True) for c in (k1, be1)]
+    # the dense restatement on the same stencils
+    n, n_sets = 33, len(idx)
+    zs = np.linspace(-0.3e-3, 0.3e-3, n)
+    vs = np.linspace(-0.1, 0.1, n)
+    v = np.tile(np.concatenate([np.zeros(n), vs]), n_sets)
+    z = np.tile(np.concatenate([zs, np.zeros(n)]), n_sets)
+    f2, p2, b2, fr2, s02 = leaves("cpu")
+    F2 = td.force(mol, kdir, pol, fr2, s02, b2, v, z, 2 * n).view(n_sets, 2 * n)
+    k2 = -(F2[:, :n] * torch.as_tensor(stencil_weights(zs))).sum(1)
+    be2 = -(F2[:, n:] * torch.as_tensor(stencil_weights(vs))).sum(1) / mol.mass
+    assert np.allclose(k1.detach().cpu().numpy(), k2.detach().numpy(), rtol=1e-9, atol=0)
+    assert np.allclose(be1.detach().cpu().numpy(), be2.detach().numpy(), rtol=1e-9, atol=0)
+    g2 = [torch.autograd.grad(c.sum(), [f2, p2, b2], retain_graph=True) for c in (k2, be2)]
+    for ga_all, gb_all in zip(g1, g2):
+        for ga, gb in zip(ga_all, gb_all):
+            ga, gb = ga.cpu().numpy().reshape(n_sets, -1), gb.numpy().reshape(n_sets, -1)
+            scale = np.abs(gb).max(axis=1, keepdims=True)
+            assert np.all(np.abs(ga - gb) <= 1e-8 * scale), float((np.abs(ga - gb) / scale).max())

@@ -97,3 +97,30 @@ def test_trajectory_gradient_parameter_maps():
         _param_map([0, 1, 2], 2, 3, "freq_par")    # one entry per beam
     import ctypes
     assert ctypes.sizeof(_lib.TgradOpts) == 8 * 7 + 4 * 2 + 4 * 2 * _lib.MM_MAX_BEAMS + 4 * 2
+
+
+def test_static_uneven_output_checks():
+    """UnevenBatch.force_static hands the caller's buffers to the kernels as
+    they are, so each must be rejected on the host when its dtype, device,
+    layout or length is wrong (no GPU needed: the checks run first)."""
+    import torch
+    from molmot_b200.uneven import check_static_out
+    dev = torch.device("cuda", 0)
+    n = 10
+    ok = torch.empty(n, dtype=torch.float64)  # right dtype and length, but on the host
+    with pytest.raises(ValueError, match="must be on cuda:0"):
+        check_static_out({"F": ok}, n, dev)
+    cpu = torch.device("cpu")  # the same rules, checked against the host device
+    check_static_out({"F": ok, "R": ok.clone(), "status": torch.zeros(n, dtype=torch.int32)}, n, cpu)
+    with pytest.raises(ValueError, match="'F'"):
+        check_static_out({}, n, cpu)
+    with pytest.raises(ValueError, match="float64"):
+        check_static_out({"F": torch.empty(n, dtype=torch.float32)}, n, cpu)
+    with pytest.raises(ValueError, match="int32"):
+        check_static_out({"F": ok, "status": torch.zeros(n, dtype=torch.int64)}, n, cpu)
+    with pytest.raises(ValueError, match="contiguous"):
+        check_static_out({"F": torch.empty(2 * n, dtype=torch.float64)[::2]}, n, cpu)
+    with pytest.raises(ValueError, match="hold 10"):
+        check_static_out({"F": torch.empty(n - 1, dtype=torch.float64)}, n, cpu)
+    with pytest.raises(ValueError, match="unknown output"):
+        check_static_out({"F": ok, "pop": ok}, n, cpu)
