@@ -7,6 +7,7 @@ Run in a container that has the reference checkout (default
     python tests/golden/make_golden.py             # SrOH fixtures
     python tests/golden/make_golden.py analysis    # analysis_golden.npz
     python tests/golden/make_golden.py molecules   # molecules_golden.npz (CaF, CaOH)
+    python tests/golden/make_golden.py force3d     # force3d_reference.npz (3D, synthetic molecules)
 
 It (1) extracts the reference's own golden arrays from
 validation/three_way_results.npz and validation/trajectory_cpu_vs_gpu_results.npz,
@@ -277,9 +278,88 @@ def molecules_golden():
     print("molecules golden written")
 
 
+def force3d_reference_golden():
+    """The reference's 3D model (molmot/mot/simulator_3d.py:168-365
+    rate_eq_force_3d, :443-504 MOTSimulator3D.simulate_trajectory_3d) run on
+    synthetic molecules whose ground Zeeman Hamiltonian has a non-degenerate
+    spectrum (molmot_b200.molecules.synthetic; the eigenbasis, and so the
+    force, is a well-posed function of the inputs): 72 (r, v) points and
+    3 leapfrog trajectories of 200 steps per molecule.  Also the reference's
+    own spread on the SrOH cases of force3d_golden.npz: the largest change of
+    its force under 1e-15 relative Hermitian perturbations of the Zeeman
+    Hamiltonian passed to numpy.linalg.eigh (6 draws per case), relative to
+    max |F| of the case.  Writes force3d_reference.npz."""
+    import importlib
+    from molmot.mot.simulator_3d import MOTSimulator3D, rate_eq_force_3d
+    from molmot.obe.obe_subdoppler import make_beam_pairs_dc4
+    sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+    from molmot_b200.molecules.synthetic import synthetic_molecule
+    out = {"versions": versions()}
+    mols = [(12, 4, 5, -0.5, 0.5, 1.0, 0.2), (8, 3, 21, -0.8, 0.3, 2.0, 0.25)]
+    out["n_mol"] = len(mols)
+    for i, (ng, ne, seed, d, sp, s0_, Bg) in enumerate(mols):
+        m = synthetic_molecule(ng, ne, seed)
+        sim = MOTSimulator3D(m, make_beam_pairs_dc4(m, d, sp, s0_), B_gradient=Bg)
+        rng = np.random.default_rng(100 + i)
+        r = np.concatenate([rng.normal(0, 3e-3, (64, 3)), np.zeros((1, 3)),
+                            [[0, 0, 2e-3], [1e-3, 0, 0], [0, -1e-3, 0], [0, 0, -4e-3],
+                             [2e-3, 2e-3, 1e-3], [-1e-3, 0.5e-3, 3e-3], [5e-3, -4e-3, 2e-3]]])
+        v = np.concatenate([rng.normal(0, 2.0, (64, 3)), np.zeros((8, 3))])
+        F = np.zeros((len(r), 3)); R = np.zeros(len(r)); P = np.zeros((len(r), ng))
+        for j in range(len(r)):
+            F[j], R[j], P[j] = rate_eq_force_3d(m, sim.beams, r[j], v[j], Bg)
+        r0 = np.array([[1e-3, -1e-3, 0.5e-3], [0.0, 0.5e-3, -2e-3], [2e-3, 1e-3, 0.0]])
+        v0 = np.array([[0.3, 0.2, -0.5], [-0.4, 0.0, 0.6], [0.0, 0.1, 0.1]])
+        trs = [sim.simulate_trajectory_3d(r0[j], v0[j], t_max=2e-4, dt=1e-6) for j in range(3)]
+        out.update({f"m{i}_ng": ng, f"m{i}_ne": ne, f"m{i}_seed": seed, f"m{i}_B": Bg,
+                    f"m{i}_pairs": np.array([d, sp, s0_]),
+                    f"m{i}_khat": np.array([b.k_hat for b in sim.beams]),
+                    f"m{i}_freq": np.array([b.freq for b in sim.beams]),
+                    f"m{i}_q": np.array([b.q_lab for b in sim.beams], dtype=np.int32),
+                    f"m{i}_s0": np.array([b.s0 for b in sim.beams]),
+                    f"m{i}_radius": np.array([b.beam_radius for b in sim.beams]),
+                    f"m{i}_r": r, f"m{i}_v": v, f"m{i}_F": F, f"m{i}_R": R, f"m{i}_P": P,
+                    f"m{i}_r0": r0, f"m{i}_v0": v0, f"m{i}_t_max": 2e-4, f"m{i}_dt": 1e-6,
+                    f"m{i}_traj_r": np.array([t[1] for t in trs]),
+                    f"m{i}_traj_v": np.array([t[2] for t in trs])})
+    # the reference's own spread on the SrOH cases
+    from molmot.molecules.sroh import load_sroh_from_julia
+    from molmot.mot.simulator_3d import Beam3D
+    mol = load_sroh_from_julia(os.path.join(REF, "julia_sim"), verbose=False)
+    g = np.load(os.path.join(HERE, "force3d_golden.npz"))
+    orig = np.linalg.eigh
+    prng = np.random.default_rng(0)
+
+    def perturbed(H):
+        E = prng.normal(size=H.shape) + 1j * prng.normal(size=H.shape)
+        return orig(H + 1e-15 * np.abs(H).max() * (E + E.conj().T) / 2)
+
+    spreads = []
+    for c in range(int(g["n_cases"])):
+        K = lambda k: g[f"c{c}_{k}"]
+        beams = [Beam3D(k_hat=K("khat")[b], freq=K("freq")[b], q_lab=int(K("q")[b]), s0=K("s0")[b],
+                        beam_radius=K("radius")[b]) for b in range(len(K("freq")))]
+        scale = np.abs(K("F")).max()
+        spread = 0.0
+        np.linalg.eigh = perturbed
+        try:
+            for _ in range(6):
+                Fp = np.array([rate_eq_force_3d(mol, beams, K("r")[j], K("v")[j], float(K("B")))[0]
+                               for j in range(len(K("r")))])
+                spread = max(spread, float(np.abs(Fp - K("F")).max() / scale))
+        finally:
+            np.linalg.eigh = orig
+        spreads.append(spread)
+    out["sroh_spread"] = np.array(spreads)
+    np.savez(os.path.join(HERE, "force3d_reference.npz"), **out)
+    print("force3d_reference.npz written; SrOH spreads", spreads)
+
+
 if __name__ == "__main__":
     if len(sys.argv) > 1 and sys.argv[1] == "analysis":
         analysis_golden()
+    elif len(sys.argv) > 1 and sys.argv[1] == "force3d":
+        force3d_reference_golden()
     elif len(sys.argv) > 1 and sys.argv[1] == "molecules":
         molecules_golden()
     else:
