@@ -129,6 +129,12 @@ MM_API int mm_beams_view(const mm_beams *parent, int32_t first_set, int32_t n_se
  * (molmot/obe/rate_equations_jit.py:18-145).
  * v, z: device arrays (layout per opts).  Outputs: F[n], R[n] (R nullable),
  * pop[n][n_ground] (nullable), status[n] (nullable), n = total points.
+ * Molecules up to MM_MAX_GROUND x MM_MAX_EXCITED: those with n_ground <= 12
+ * and n_excited <= 4 run the register-resident kernels; larger ones run
+ * shared-memory kernels (a group of 16 or 32 lanes per point) in FP64 for
+ * every precision -- the reference's elimination for MM_PREC_FP64, the
+ * excited-chain solve for the other precisions when every set passes its
+ * structural checks (else the elimination).
  */
 MM_API int mm_force_batch(const mm_pack *pack, const mm_beams *beams, const double *v,
                    const double *z, int64_t n_points, const mm_batch_opts *opts,
@@ -148,6 +154,8 @@ MM_API int mm_force_batch(const mm_pack *pack, const mm_beams *beams, const doub
  * MM_PREC_FP64_REDUCED (the adjoint of the excited-chain solve, one point per
  * thread; when any set fails the reduced form's structural checks the whole
  * batch runs the elimination adjoint).  Other precisions are rejected.
+ * Molecules beyond n_ground 12 / n_excited 4 run the elimination adjoint in
+ * shared memory (group of 16 or 32 lanes per point) for both precisions.
  */
 MM_API int mm_force_adjoint(const mm_pack *pack, const mm_beams *beams, const double *v,
                             const double *z, int64_t n_points, const mm_batch_opts *opts,
@@ -234,6 +242,8 @@ typedef struct {
  * with vsq_sum / n_samp it also accumulates the sums of monte_carlo_temperature
  * (molmot/propagation/trajectories.py:159-229).  Arrays are [N][ndim]
  * (r_traj / v_traj: [N][n_steps][ndim], nullable; vsq_sum / n_samp: [N], nullable).
+ * Molecules beyond n_ground 12 / n_excited 4 run the plain FP64 force in
+ * shared memory (group of 16 or 32 lanes per particle) for both precisions.
  */
 MM_API int mm_traj_run(const mm_pack *pack, const mm_beams *beams, const mm_traj_opts *opts,
                        const double *r0, const double *v0, int64_t n_particles,
@@ -271,7 +281,9 @@ typedef struct {
  * (nullable): the state after steps ckpt_every, 2 ckpt_every, ... of the call;
  * passing checkpoint c back as state with step0 + (c + 1) ckpt_every resumes
  * the run bit for bit.  Beam set 0 must pass the reduced form's structural
- * checks (every ground state pumped, excited chain strongly connected).
+ * checks (every ground state pumped, excited chain strongly connected), and
+ * the molecule must fit the register-resident class (n_ground <= 12,
+ * n_excited <= 4).
  */
 MM_API int mm_traj_grad_run(const mm_pack *pack, const mm_beams *beams, const mm_tgrad_opts *opts,
                             int64_t n_particles, double *state, int32_t *n_actual, double *ckpt,
@@ -296,7 +308,7 @@ MM_API int mm_traj1d_run(const mm_pack *pack, const mm_beams *beams, const doubl
  * (molmot/mot/simulator_3d.py:168-365) and rate_eq_force_3d_batch
  * (molmot_cuda/simulator_3d_cuda.py:666-754; that kernel's Jacobi eigensolver
  * is replaced by a correct one).  Needs a pack with the 3D fields and beam
- * sets with khat.  hbar <= 0 selects CODATA 1.054571817e-34 (the 3D
+ * sets with khat; molecules up to 16 ground and 8 excited states.  hbar <= 0 selects CODATA 1.054571817e-34 (the 3D
  * reference path's value).  Outputs: F[n][3], R[n] (nullable),
  * pop[n][n_ground] (nullable), status[n] (nullable).
  */

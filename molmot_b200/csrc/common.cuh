@@ -66,6 +66,20 @@ struct ForceParams {
     int uniform_fb;
 };
 
+// Parameters of the fused 1D trajectory kernels (passed by value).
+struct TrajParams {
+    double dt, z_escape, mass;
+    long long n_particles, n_steps;
+    int ndim;         // 1: along z;  3: per-axis model (x, y, z)
+    int n_avg;        // parameter sets averaged per force evaluation (RF MOT: 2 phases)
+    long long i_eq;   // first step whose v^2 enters vsq_sum (temperature); < 0: off
+    const double *z0, *v0;          // [N][ndim]
+    double *z_final, *v_final;      // [N][ndim]
+    double *z_traj, *v_traj;        // [N][n_steps][ndim] or null
+    int32_t *n_actual;              // [N]
+    double *vsq_sum, *n_samp;       // [N] or null
+};
+
 __device__ __forceinline__ double mm_group_sum(double x, int G)
 {
     for (int o = G >> 1; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);

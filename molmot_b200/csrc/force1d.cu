@@ -18,6 +18,7 @@
 #include "rate_core.cuh"
 #include "reduced.cuh"
 #include "kicks.cuh"
+#include "large.cuh"
 
 namespace {
 
@@ -316,18 +317,6 @@ force_reduced_adjoint_kernel(ForceParams P, double *grad)
     }
 }
 
-struct TrajParams {
-    double dt, z_escape, mass;
-    long long n_particles, n_steps;
-    int ndim;         // 1: along z;  3: per-axis model (x, y, z)
-    int n_avg;        // parameter sets averaged per force evaluation (RF MOT: 2 phases)
-    long long i_eq;   // first step whose v^2 enters vsq_sum (temperature); < 0: off
-    const double *z0, *v0;          // [N][ndim]
-    double *z_final, *v_final;      // [N][ndim]
-    double *z_traj, *v_traj;        // [N][n_steps][ndim] or null
-    int32_t *n_actual;              // [N]
-    double *vsq_sum, *n_samp;       // [N] or null
-};
 
 // Fused trajectories, one particle per group, all steps in one launch.
 //  ndim = 1: symplectic Euler along z (molmot/propagation/trajectories_jit.py:18-58,
@@ -901,8 +890,8 @@ int dispatch_class(int n_g, int n_e, F &&f)
 {
     if (n_g == 12 && n_e == 4) return f(Class<12, 4, 4, true>{});   // SrOH
     if (n_g <= 12 && n_e <= 4) return f(Class<12, 4, 4, false>{});
-    mm_set_error("molecule size n_ground=%d n_excited=%d exceeds the register-resident 1D "
-                 "kernel class (n_ground <= 12, n_excited <= 4)", n_g, n_e);
+    mm_set_error("molecule size n_ground=%d n_excited=%d: this entry point runs the register-"
+                 "resident kernels only (n_ground <= 12, n_excited <= 4)", n_g, n_e);
     return -1;
 }
 
@@ -947,6 +936,8 @@ extern "C" int mm_force_adjoint(const mm_pack *pack, const mm_beams *beams, cons
     }
     P.R = nullptr; P.pop = nullptr; P.status = nullptr;
     cudaStream_t st = (cudaStream_t)stream;
+    // beyond the register classes: the shared-memory elimination adjoint (both precisions)
+    if (!mm_register_class(P.n_g, P.n_e)) return mm_large_adjoint(P, pps, grad, st);
     // FP64-reduced: the reduced adjoint when every set is structurally valid,
     // else the elimination adjoint for the whole batch
     const bool red = opts->precision == MM_PREC_FP64_REDUCED && reduced_all_valid(pack, beams);
@@ -1012,6 +1003,11 @@ extern "C" int mm_force_batch(const mm_pack *pack, const mm_beams *beams, const 
     P.R = R; P.pop = pop; P.status = status;
     const int prec = opts->precision;
     cudaStream_t st = (cudaStream_t)stream;
+    // beyond the register classes: the shared-memory kernels in FP64 for every
+    // precision (the plain form's elimination, or the excited-chain solve for
+    // the other forms when every set passes its structural checks)
+    if (!mm_register_class(P.n_g, P.n_e))
+        return mm_large_force(P, pps, prec != MM_PREC_FP64 && reduced_all_valid(pack, beams), st);
     return dispatch_class(P.n_g, P.n_e, [&](auto C) -> int {
         using CT = decltype(C);
         if (prec == MM_PREC_FP64) return launch_force<CT>(P, pps, st);
@@ -1061,6 +1057,8 @@ extern "C" int mm_traj_run(const mm_pack *pack, const mm_beams *beams, const mm_
     T.vsq_sum = vsq_sum; T.n_samp = n_samp;
     const bool fp32 = topt->precision == MM_PREC_FP32_REFINE;
     cudaStream_t st = (cudaStream_t)stream;
+    // beyond the register classes: the plain FP64 force from the shared-memory kernel
+    if (!mm_register_class(P.n_g, P.n_e)) return mm_large_traj(P, T, st);
     return dispatch_class(P.n_g, P.n_e, [&](auto C) -> int {
         using CT = decltype(C);
         if (!fp32) return launch_traj<CT>(P, T, st);

@@ -31,11 +31,17 @@
 namespace {
 
 constexpr int kG3 = 16;        // lanes per point
-constexpr int kThreads3 = 128; // 8 points per CTA
-constexpr int NGM = 12;        // max ground states of the 3D kernel (SrOH-sized)
-constexpr int NEM = 4;         // max excited states
 constexpr int NBM = 32;        // max beams
-constexpr int LDH = NGM + 1;   // padded row length of the matrices in shared memory
+
+// Size classes of the 3D kernels: NGM ground and NEM excited states at most,
+// THREADS per CTA (8 points per CTA for SrOH-sized molecules, 4 for the
+// larger class, whose per-point tables are twice as large).
+template <int NGM_, int NEM_, int THREADS_>
+struct C3 {
+    static constexpr int NGM = NGM_, NEM = NEM_, THREADS = THREADS_;
+};
+using C3Small = C3<12, 4, 128>;
+using C3Large = C3<16, 8, 64>;
 
 struct Force3Params {
     int n_g, n_e, n_b, n_sets;
@@ -64,14 +70,20 @@ struct Traj3Params {
 };
 
 // Per-CTA constants (molecule + one beam set) and per-group work arrays.
+// The two 16-lane groups of a warp read the same offsets of their own
+// Group (rotation coefficients, beam terms, ...).  Groups that sit 16 banks
+// apart (sizeof % 128 == 64) make those pairs of reads conflict-free; a
+// multiple of 128 bytes would put both in the same banks.
+template <int NGM, int NEM, int THREADS>
 struct Smem3 {
+    static constexpr int LDH = NGM + 1;  // padded row length of the matrices
     double Zre[3][NGM * NGM], Zim[3][NGM * NGM];
     double tdm[NGM * NEM * 3];
     double E[NGM + NEM], Ze[NEM];
     double khat[NBM][3], freq[NBM], s0[NBM], radius[NBM];
     int pol[NBM];
     unsigned short sched[NGM - 1][NGM / 2];  // circle schedule: p | q << 8 of round r, slot i
-    struct Group {
+    struct GroupBody {
         double Hre[NGM * LDH], Him[NGM * LDH];
         double Vre[NGM * LDH], Vim[NGM * LDH];
         double rot[NGM / 2][3];      // c, Re s, Im s
@@ -81,15 +93,14 @@ struct Smem3 {
         double BR[NEM * NGM];
         double Esg[NGM], Ese[NEM];
         double bm[NBM][5];           // doppler, s_eff, w0, w1, w2
-        double pad_[4];              // see the size check below
-    } grp[kThreads3 / kG3];
+    };
+    static constexpr size_t kPad = (64 + 128 - sizeof(GroupBody) % 128) % 128;
+    struct Group : GroupBody {
+        unsigned char pad_[kPad == 0 ? 128 : kPad];
+    };
+    static_assert(sizeof(Group) % 128 == 64, "Group stride must be 16 banks off a 128-byte multiple");
+    Group grp[THREADS / kG3];
 };
-
-// The two 16-lane groups of a warp read the same offsets of their own
-// Group (rotation coefficients, beam terms, ...).  Groups that sit 16 banks
-// apart (sizeof % 128 == 64) make those pairs of reads conflict-free; a
-// multiple of 128 bytes would put both in the same banks.
-static_assert(sizeof(Smem3::Group) % 128 == 64, "Group stride must be 16 banks off a 128-byte multiple");
 
 __device__ __forceinline__ double gsum16(double x)
 {
@@ -101,12 +112,14 @@ __device__ __forceinline__ double gsum16(double x)
 
 // Player at position j in round r of the circle schedule on NGM players:
 // position 0 stays, the others rotate; slot i pairs positions i and NGM-1-i.
+template <int NGM>
 __host__ __device__ constexpr int rr_player(int r, int j)
 {
     return j == 0 ? 0 : ((r + j - 1) % (NGM - 1)) + 1;
 }
 
-__device__ void load_consts3(const Force3Params &P, int set, Smem3 &S)
+template <int NGM, int NEM, int TH>
+__device__ void load_consts3(const Force3Params &P, int set, Smem3<NGM, NEM, TH> &S)
 {
     const int n_g = P.n_g, n_e = P.n_e, n_b = P.n_b, tid = threadIdx.x, nt = blockDim.x;
     for (int i = tid; i < 3 * n_g * n_g; i += nt) {
@@ -117,7 +130,7 @@ __device__ void load_consts3(const Force3Params &P, int set, Smem3 &S)
     for (int i = tid; i < n_g * n_e * 3; i += nt) S.tdm[i] = P.tdm[i];
     for (int i = tid; i < (NGM - 1) * (NGM / 2); i += nt) {
         const int r = i / (NGM / 2), k = i % (NGM / 2);
-        S.sched[r][k] = (unsigned short)(rr_player(r, k) | rr_player(r, NGM - 1 - k) << 8);
+        S.sched[r][k] = (unsigned short)(rr_player<NGM>(r, k) | rr_player<NGM>(r, NGM - 1 - k) << 8);
     }
     for (int i = tid; i < n_g + n_e; i += nt) S.E[i] = P.E[i];
     for (int i = tid; i < n_e; i += nt) S.Ze[i] = P.Ze[i];
@@ -144,9 +157,10 @@ struct Out3 {
 // pair) and column t of H (rows p, q).  The round index is a run-time value
 // (one copy of this code serves the NGM - 1 rounds); the pair loop is
 // unrolled.
-__device__ __forceinline__ void jacobi_round(Smem3::Group &W, int t, const unsigned short *pq)
+template <int NGM, class GroupT>
+__device__ __forceinline__ void jacobi_round(GroupT &W, int t, const unsigned short *pq)
 {
-    constexpr int NP = NGM / 2;
+    constexpr int NP = NGM / 2, LDH = NGM + 1;
     if (t < NP) {
         const int p = pq[t] & 0xff, q = pq[t] >> 8;
         double c = 1.0, sr = 0.0, si = 0.0;
@@ -215,9 +229,12 @@ __device__ __forceinline__ void jacobi_round(Smem3::Group &W, int t, const unsig
 
 // The 3D force at (r, v) for the group of 16 lanes (lane t, base gbase).
 // pl receives the population of ground state t (t < n_g).
-__device__ Out3 force3d_point(const Force3Params &P, Smem3 &S, Smem3::Group &W, int t, int gbase,
+template <int NGM, int NEM, int TH>
+__device__ Out3 force3d_point(const Force3Params &P, Smem3<NGM, NEM, TH> &S,
+                              typename Smem3<NGM, NEM, TH>::Group &W, int t, int gbase,
                               const double r[3], const double v[3], double Bg, double &pl)
 {
+    constexpr int LDH = NGM + 1;
     constexpr unsigned FULL = 0xffffffffu;
     const int n_g = P.n_g, n_e = P.n_e, n_b = P.n_b;
     const double G = P.Gamma;
@@ -270,7 +287,7 @@ __device__ Out3 force3d_point(const Force3Params &P, Smem3 &S, Smem3::Group &W, 
         const bool more = off > 1e-30 * dia && off > 1e-300;
         if (!__any_sync(FULL, more)) break;
 #pragma unroll 1
-        for (int rnd = 0; rnd < NGM - 1; rnd++) jacobi_round(W, t, S.sched[rnd]);
+        for (int rnd = 0; rnd < NGM - 1; rnd++) jacobi_round<NGM>(W, t, S.sched[rnd]);
     }
     // ascending order (ties by index), as eigh returns the spectrum
     if (t < n_g) {
@@ -468,13 +485,14 @@ __device__ Out3 force3d_point(const Force3Params &P, Smem3 &S, Smem3::Group &W, 
     return o;
 }
 
-__global__ void __launch_bounds__(kThreads3)
+template <int NGM, int NEM, int TH>
+__global__ void __launch_bounds__(TH)
 force3d_kernel(Force3Params P)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
-    Smem3 &S = *reinterpret_cast<Smem3 *>(smraw);
+    auto &S = *reinterpret_cast<Smem3<NGM, NEM, TH> *>(smraw);
     const int lane = threadIdx.x & 31, t = lane % kG3, gbase = lane - t;
-    const int group = threadIdx.x / kG3, ngroups = kThreads3 / kG3;
+    const int group = threadIdx.x / kG3, ngroups = TH / kG3;
     for (int set = blockIdx.y; set < P.n_sets; set += gridDim.y) {
         const long long first = (long long)set * P.pps;
         long long count = P.pps;
@@ -508,13 +526,14 @@ force3d_kernel(Force3Params P)
 //   v_1/2 = v_0 + (0.5 dt) F(r_0, v_0)/m;  r_j = r_{j-1} + dt v_half;
 //   escape when |r_j| > r_escape (position and half-step velocity freeze);
 //   F = F(r_j, v_half); v_new = v_half + dt F/m (+ recoil kick); v_j = (v_half + v_new)/2.
-__global__ void __launch_bounds__(kThreads3)
+template <int NGM, int NEM, int TH>
+__global__ void __launch_bounds__(TH)
 traj3d_kernel(Force3Params P, Traj3Params T)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
-    Smem3 &S = *reinterpret_cast<Smem3 *>(smraw);
+    auto &S = *reinterpret_cast<Smem3<NGM, NEM, TH> *>(smraw);
     const int lane = threadIdx.x & 31, t = lane % kG3, gbase = lane - t;
-    const int group = threadIdx.x / kG3, ngroups = kThreads3 / kG3;
+    const int group = threadIdx.x / kG3, ngroups = TH / kG3;
     load_consts3(P, 0, S);
     __syncthreads();
     const double Bg = P.bgrad[0];
@@ -591,9 +610,9 @@ int fill3(const mm_pack *pack, const mm_beams *beams, double hbar, int uniform_f
     if (!pack || !beams) { mm_set_error("null pack or beams handle"); return -1; }
     if (!pack->has3d) { mm_set_error("the molecule pack has no 3D data (Zeeman blocks, |tdm|)"); return -1; }
     if (!beams->has3d) { mm_set_error("the beam sets have no 3D data (khat)"); return -1; }
-    if (pack->n_g > NGM || pack->n_e > NEM) {
-        mm_set_error("3D kernel supports n_ground <= %d, n_excited <= %d (got %d, %d)", NGM, NEM,
-                     pack->n_g, pack->n_e);
+    if (pack->n_g > C3Large::NGM || pack->n_e > C3Large::NEM) {
+        mm_set_error("3D kernel supports n_ground <= %d, n_excited <= %d (got %d, %d)", C3Large::NGM,
+                     C3Large::NEM, pack->n_g, pack->n_e);
         return -1;
     }
     if (beams->n_b > NBM) { mm_set_error("3D kernel supports <= %d beams", NBM); return -1; }
@@ -610,11 +629,49 @@ int fill3(const mm_pack *pack, const mm_beams *beams, double hbar, int uniform_f
 }
 
 template <class K>
-int prep_smem(K kern)
+int prep_smem(K kern, size_t sb)
 {
-    const int sb = (int)sizeof(Smem3);
-    return mm_cuda_check(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, sb),
+    return mm_cuda_check(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb),
                          "cudaFuncSetAttribute") ? -3 : 0;
+}
+
+// The 3D size class of a molecule: SrOH-sized (12 + 4) or the larger one (16 + 8).
+template <class F>
+int dispatch3(int n_g, int n_e, F &&f)
+{
+    if (n_g <= C3Small::NGM && n_e <= C3Small::NEM) return f(C3Small{});
+    return f(C3Large{});
+}
+
+template <class C>
+int launch_force3d(const Force3Params &P, long long n_points, long long pps, cudaStream_t st)
+{
+    auto kern = force3d_kernel<C::NGM, C::NEM, C::THREADS>;
+    const size_t sb = sizeof(Smem3<C::NGM, C::NEM, C::THREADS>);
+    if (prep_smem(kern, sb)) return -3;
+    int dev = 0, nsm = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, C::THREADS, sb);
+    const int ngroups = C::THREADS / kG3;
+    const int n_sets_used = (int)((n_points + pps - 1) / pps);
+    long long gx = std::max<long long>(1, (long long)nsm * std::max(per_sm, 1) * 2 / n_sets_used);
+    gx = std::min<long long>(gx, (pps + ngroups - 1) / ngroups);
+    dim3 grid((unsigned)gx, (unsigned)std::min(n_sets_used, 65535));
+    kern<<<grid, C::THREADS, sb, st>>>(P);
+    return mm_cuda_check(cudaGetLastError(), "force3d_kernel launch") ? -3 : 0;
+}
+
+template <class C>
+int launch_traj3d(const Force3Params &P, const Traj3Params &T, cudaStream_t st)
+{
+    auto kern = traj3d_kernel<C::NGM, C::NEM, C::THREADS>;
+    const size_t sb = sizeof(Smem3<C::NGM, C::NEM, C::THREADS>);
+    if (prep_smem(kern, sb)) return -3;
+    const int ngroups = C::THREADS / kG3;
+    const long long gx = (T.n_particles + ngroups - 1) / ngroups;
+    kern<<<(unsigned)gx, C::THREADS, sb, st>>>(P, T);
+    return mm_cuda_check(cudaGetLastError(), "traj3d_kernel launch") ? -3 : 0;
 }
 
 }  // namespace
@@ -637,18 +694,9 @@ extern "C" int mm_force3d_batch(const mm_pack *pack, const mm_beams *beams, cons
     }
     P.n_points = n_points; P.pps = pps; P.r = r; P.v = v; P.F = F; P.R = R; P.pop = pop;
     P.status = status;
-    if (prep_smem(force3d_kernel)) return -3;
-    int dev = 0, nsm = 148, per_sm = 1;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, force3d_kernel, kThreads3, sizeof(Smem3));
-    const int ngroups = kThreads3 / kG3;
-    const int n_sets_used = (int)((n_points + pps - 1) / pps);
-    long long gx = std::max<long long>(1, (long long)nsm * std::max(per_sm, 1) * 2 / n_sets_used);
-    gx = std::min<long long>(gx, (pps + ngroups - 1) / ngroups);
-    dim3 grid((unsigned)gx, (unsigned)std::min(n_sets_used, 65535));
-    force3d_kernel<<<grid, kThreads3, sizeof(Smem3), (cudaStream_t)stream>>>(P);
-    return mm_cuda_check(cudaGetLastError(), "force3d_kernel launch") ? -3 : 0;
+    return dispatch3(P.n_g, P.n_e, [&](auto C) -> int {
+        return launch_force3d<decltype(C)>(P, n_points, pps, (cudaStream_t)stream);
+    });
 }
 
 extern "C" int mm_traj3d_run(const mm_pack *pack, const mm_beams *beams, const double *r0,
@@ -681,9 +729,7 @@ extern "C" int mm_traj3d_run(const mm_pack *pack, const mm_beams *beams, const d
     T.r0 = r0; T.v0 = v0; T.r_out = r_out; T.vh_out = vh_out; T.v_out = v_out;
     T.n_actual = n_actual; T.r_traj = r_traj; T.v_traj = v_traj; T.ke_sum = ke;
     T.n_events = n_events;
-    if (prep_smem(traj3d_kernel)) return -3;
-    const int ngroups = kThreads3 / kG3;
-    const long long gx = (n_particles + ngroups - 1) / ngroups;
-    traj3d_kernel<<<(unsigned)gx, kThreads3, sizeof(Smem3), (cudaStream_t)stream>>>(P, T);
-    return mm_cuda_check(cudaGetLastError(), "traj3d_kernel launch") ? -3 : 0;
+    return dispatch3(P.n_g, P.n_e, [&](auto C) -> int {
+        return launch_traj3d<decltype(C)>(P, T, (cudaStream_t)stream);
+    });
 }

@@ -19,7 +19,7 @@
 #include <string.h>
 #include <algorithm>
 #include <vector>
-#include "rate_core.cuh"
+#include "smem_solve.cuh"
 
 struct mm_bank {
     int n_mol;
@@ -51,8 +51,6 @@ struct mm_uneven_plan {
 
 namespace {
 
-constexpr int NBU = MM_MAX_BEAMS;
-
 struct UnevenParams {
     const int *ng, *ne;
     const long long *off;
@@ -77,76 +75,34 @@ struct UnevenParams {
 
 template <int NGMAX, int NEMAX, bool RED = false>
 struct ULayout {
-    static constexpr int LDA = NGMAX + 1;
-    static constexpr int LDK = NEMAX + 1;
-    // row stride of the rates Rm[g][e]: lanes own consecutive ground states,
-    // so an odd stride keeps their row accesses in distinct banks
-    static constexpr int LDR = NEMAX + 1;
-    // per CTA
-    static constexpr int mol_doubles = 2 * (NGMAX + NEMAX) + NGMAX * NEMAX * 3 + NEMAX * NGMAX + NGMAX;
-    static constexpr int beam_doubles = 5 * NBU;
-    // per group
-    // elimination: A, Rm, bv, xv, invU, Fk, Rk, Esg, fd, Ese
-    // reduced:     Rm (scaled rates), K, Fk, Rk, Esg, w, phi, fd, Ese, cw, cf, rs, pi
-    static constexpr int grp_raw = RED ? NGMAX * LDR + NEMAX * LDK + 5 * NGMAX + NBU + 5 * NEMAX
-                                       : NGMAX * LDA + NGMAX * LDR + 6 * NGMAX + NBU + NEMAX;
-    // two 16-lane groups of a warp read the same offsets of their own region:
-    // a stride of 16 banks past a multiple of 128 bytes keeps those reads
-    // conflict-free (a multiple of 128 bytes would put both in the same banks)
-    static constexpr int grp_doubles = (grp_raw + 15) / 16 * 16 + 8;
+    using W = SmWorkLayout<NGMAX, NEMAX, RED>;
+    static constexpr int mol_doubles = SmMolLayout<NGMAX, NEMAX>::doubles;
     static size_t bytes(int groups)
     {
-        return sizeof(double) * (size_t)(mol_doubles + beam_doubles + groups * grp_doubles) +
-               sizeof(int) * (NBU + 8);
+        return sizeof(double) * (size_t)(mol_doubles + kSmBeamDoubles + groups * W::doubles) +
+               sizeof(int) * (kSmBeamInts + 8);
     }
 };
 
-__device__ __forceinline__ double gsum(double x, int G)
-{
-    for (int o = G >> 1; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-    return x;
-}
-
 // RED: the populations from the excited-state chain (see reduced.cuh for the
-// identity): each group scales its rates by 1/r_g, forms K = A^T BR^T
-// (n_e x n_e) and the two n_e-vectors in shared memory, reduces the chain
-// cooperatively and writes F and R.  Molecules the reduction does not cover
-// (valid[m] = 0) are left to the elimination kernels (RED = false).
+// identity).  Molecules the reduction does not cover (valid[m] = 0) are left
+// to the elimination kernels (RED = false).  The point solve is sm_point
+// (smem_solve.cuh).
 template <int NGMAX, int NEMAX, int G, bool RED>
 __global__ void __launch_bounds__(256)
 uneven_kernel(UnevenParams P)
 {
     using Ly = ULayout<NGMAX, NEMAX, RED>;
-    constexpr int LDA = Ly::LDA, LDK = Ly::LDK, LDR = Ly::LDR;
     extern __shared__ __align__(16) unsigned char smraw[];
     double *smd = (double *)smraw;
-    // molecule
-    double *E = smd, *zd = E + NGMAX + NEMAX, *d2s = zd + NGMAX + NEMAX;
-    double *BR = d2s + NGMAX * NEMAX * 3, *czd = BR + NEMAX * NGMAX;
-    // beams
-    double *freq = czd + NGMAX, *ck = freq + NBU, *hk = ck + NBU, *s0 = hk + NBU, *c1 = s0 + NBU;
+    double *molsm = smd, *beamsm = molsm + Ly::mol_doubles, *grp0 = beamsm + kSmBeamDoubles;
     const int groups = blockDim.x / G;
-    double *grp0 = c1 + NBU;
-    int *pol = (int *)(grp0 + (size_t)groups * Ly::grp_doubles);
-    int *sint = pol + NBU;  // [0] task, [1] n_g, [2] n_e
+    int *pol = (int *)(grp0 + (size_t)groups * Ly::W::doubles);
+    int *sint = pol + kSmBeamInts;  // [0] task
 
     const int lane = threadIdx.x & 31, t = lane % G;
     const int group = threadIdx.x / G;
-    double *W = grp0 + (size_t)group * Ly::grp_doubles;
-    double *A, *Rm, *bv, *xv, *invU, *Fk, *Rk, *Esg, *fd, *Ese;
-    double *Kc = nullptr, *wg = nullptr, *ph = nullptr, *cw = nullptr, *cf = nullptr, *rsv = nullptr,
-           *piv = nullptr;
-    if constexpr (RED) {
-        Rm = W; Kc = Rm + NGMAX * LDR; Fk = Kc + NEMAX * LDK; Rk = Fk + NGMAX; Esg = Rk + NGMAX;
-        wg = Esg + NGMAX; ph = wg + NGMAX; fd = ph + NGMAX; Ese = fd + NBU;
-        cw = Ese + NEMAX; cf = cw + NEMAX; rsv = cf + NEMAX; piv = rsv + NEMAX;
-        A = bv = xv = invU = nullptr;
-    } else {
-        A = W; Rm = A + NGMAX * LDA; bv = Rm + NGMAX * LDR; xv = bv + NGMAX;
-        invU = xv + NGMAX; Fk = invU + NGMAX; Rk = Fk + NGMAX; Esg = Rk + NGMAX;
-        fd = Esg + NGMAX; Ese = fd + NBU;
-    }
-    const int n_b = P.n_b;
+    const SmWork W = sm_work<NGMAX, NEMAX, RED>(grp0 + (size_t)group * Ly::W::doubles, nullptr);
 
     for (int it = 0;; it++) {
         __syncthreads();
@@ -158,252 +114,23 @@ uneven_kernel(UnevenParams P)
         const UnevenTask T = P.tasks[task];
         const int m = T.mol;
         if (P.valid && (RED ? !P.valid[m] : P.valid[m])) continue;  // uniform over the CTA
-        const int n_g = P.ng[m], n_e = P.ne[m], n_s = n_g + n_e;
-        const double Gam = P.gam[m], kw = P.kw[m];
-        const double *mb = P.buf + P.off[m];
-        for (int i = threadIdx.x; i < n_s; i += blockDim.x) { E[i] = mb[i]; zd[i] = mb[n_s + i]; }
-        // |d|^2 transposed to [e][q][g]: the lanes of a group own consecutive
-        // ground states, so their reads of one (e, q) are consecutive doubles
-        for (int i = threadIdx.x; i < n_g * n_e * 3; i += blockDim.x) {
-            const int k = i / (n_e * 3), r = i - k * (n_e * 3);
-            d2s[r * NGMAX + k] = mb[2 * n_s + i];  // r = e * 3 + q
-        }
-        // branching ratios transposed to [g][e]: the chain build's lanes read
-        // consecutive excited states of one ground state
-        for (int i = threadIdx.x; i < n_e * n_g; i += blockDim.x) {
-            const int e = i / n_g, g = i - e * n_g;
-            BR[g * NEMAX + e] = mb[2 * n_s + n_g * n_e * 3 + i];
-        }
-        for (int i = threadIdx.x; i < n_g; i += blockDim.x) czd[i] = mb[n_s + i] * Gam / MM_TWO_PI;
-        const double gh = Gam / 2.0, gh2 = gh * gh;
-        for (int b = threadIdx.x; b < n_b; b += blockDim.x) {
-            const size_t o = (size_t)m * n_b + b;
-            freq[b] = P.freq[o];
-            ck[b] = __dmul_rn(-kw, P.kdir[o]);
-            hk[b] = __dmul_rn(__dmul_rn(P.hbar, kw), P.kdir[o]);
-            s0[b] = P.s0[o];
-            c1[b] = __dmul_rn(gh, P.s0[o]);
-            pol[b] = P.pol[o];
-        }
+        SmMol M;
+        SmBeam Bm;
+        sm_stage_mol<NGMAX, NEMAX>(P.buf + P.off[m], P.ng[m], P.ne[m], P.gam[m], molsm, M);
+        const size_t o = (size_t)m * P.n_b;
+        sm_stage_beams(P.kdir + o, P.freq + o, P.s0 + o, P.pol + o, P.n_b, P.bgrad[m], P.kw[m], P.hbar,
+                       P.gam[m], beamsm, pol, Bm);
         __syncthreads();
-        const double Bg = P.bgrad[m];
-
         for (long long base = T.p0; base < T.p1; base += groups) {
             const long long ip = base + group;
             const bool valid = ip < T.p1;
             const long long gi = valid ? ip : T.p0;
-            const double v = P.v[gi], z = P.z[gi];
-            int stat = 0;
-            const double B = __dmul_rn(__dmul_rn(Bg, z), 1e4);
-            __syncwarp();
-            for (int b = t; b < n_b; b += G)
-                fd[b] = __dadd_rn(freq[b], __ddiv_rn(__dmul_rn(ck[b], v), MM_TWO_PI));
-            for (int e = t; e < n_e; e += G)
-                Ese[e] = __dadd_rn(E[n_g + e], __ddiv_rn(__dmul_rn(__dmul_rn(B, zd[n_g + e]), Gam), MM_TWO_PI));
-            for (int k = t; k < n_g; k += G) Esg[k] = fma(B, czd[k], E[k]);
-            __syncwarp();
-            // rates of ground states k = t, t + G, ... (rows of Rm owned by this lane)
-            for (int k = t; k < n_g; k += G) {
-                double s = 0.0, f = 0.0;
-                double Racc[NEMAX];  // per excited state, in registers (compile-time index)
-#pragma unroll
-                for (int e = 0; e < NEMAX; e++) Racc[e] = 0.0;
-                const double Eg = Esg[k];
-                for (int b = 0; b < n_b; b++) {
-                    const int q = pol[b];
-                    const double fdb = fd[b], c1b = c1[b], hkb = hk[b], s0b = s0[b];
-#pragma unroll
-                    for (int e = 0; e < NEMAX; e++) {
-                        if (e >= n_e) break;
-                        const double d2 = d2s[(e * 3 + q) * NGMAX + k];
-                        if (d2 < 1e-15) continue;
-                        const double om = __dsub_rn(Ese[e], Eg);
-                        const double de = __dmul_rn(__dsub_rn(fdb, om), MM_TWO_PI);
-                        const double L = gh2 * mm_rcp(fma(de, de, gh2));
-                        const double ru = c1b * d2 * P.geff * L;
-                        Racc[e] += ru;
-                        f = fma(hkb, ru, f);
-                        s = fma(s0b * d2, L, s);
-                    }
-                }
-                const double sat = mm_rcp(1.0 + s);
-                double rs = 0.0;
-#pragma unroll
-                for (int e = 0; e < NEMAX; e++) {
-                    if (e < n_e) {
-                        const double r = Racc[e] * sat;
-                        Rm[k * LDR + e] = r;
-                        rs += r;
-                    }
-                }
-                Fk[k] = f * sat;
-                Rk[k] = rs;
-            }
-            __syncwarp();
-            if constexpr (RED) {
-                // a_ge = R[g,e] / r_g, w_g = 1 / r_g, phi_g = F_g / r_g (lane per ground state)
-                for (int k = t; k < n_g; k += G) {
-                    const double inv = mm_rcp(Rk[k]);  // r_g > 0: every ground state is pumped
-                    for (int e = 0; e < n_e; e++) Rm[k * LDR + e] *= inv;
-                    wg[k] = inv;
-                    ph[k] = Fk[k] * inv;
-                }
-                __syncwarp();
-                // K[e][e'] = sum_g a_ge BR[e', g]; cw, cf, rs: sums of BR[e', g] w_g, phi_g, 1
-                for (int idx = t; idx < n_e * n_e; idx += G) {
-                    const int e = idx / n_e, e2 = idx - e * n_e;
-                    double a = 0.0;
-                    for (int g = 0; g < n_g; g++) a = fma(Rm[g * LDR + e], BR[g * NEMAX + e2], a);
-                    Kc[e * LDK + e2] = a;
-                }
-                for (int e2 = t; e2 < n_e; e2 += G) {
-                    double a = 0.0, b = 0.0, c = 0.0;
-                    for (int g = 0; g < n_g; g++) {
-                        const double br = BR[g * NEMAX + e2];
-                        a = fma(br, wg[g], a);
-                        b = fma(br, ph[g], b);
-                        c += br;
-                    }
-                    cw[e2] = a;
-                    cf[e2] = b;
-                    rsv[e2] = c;
-                }
-                __syncwarp();
-                // state reduction of the chain, Q[i][j] = K[j][i] (probability i -> j)
-                bool ok = true;
-                for (int k = n_e - 1; k >= 1; k--) {
-                    double S = 0.0;
-                    for (int j = 0; j < k; j++) S += Kc[j * LDK + k];
-                    ok = ok && (S > 0.0);
-                    const double inv = mm_rcp(S > 0.0 ? S : 1.0);
-                    __syncwarp();
-                    for (int i = t; i < k; i += G) Kc[k * LDK + i] *= inv;
-                    __syncwarp();
-                    for (int idx = t; idx < k * k; idx += G) {
-                        const int i = idx / k, j = idx - i * k;
-                        Kc[j * LDK + i] = fma(Kc[k * LDK + i], Kc[j * LDK + k], Kc[j * LDK + i]);
-                    }
-                    __syncwarp();
-                }
-                double nrm = 0.0, fn = 0.0, rn = 0.0;
-                if (t == 0) {
-                    piv[0] = 1.0;
-                    for (int k = 1; k < n_e; k++) {
-                        double a = 0.0;
-                        for (int i = 0; i < k; i++) a = fma(piv[i], Kc[k * LDK + i], a);
-                        piv[k] = a;
-                    }
-                    for (int e = 0; e < n_e; e++) {
-                        nrm = fma(cw[e], piv[e], nrm);
-                        fn = fma(cf[e], piv[e], fn);
-                        rn = fma(rsv[e], piv[e], rn);
-                    }
-                    const double in = mm_rcp(nrm);
-                    const double Fo = fn * in, Ro = rn * in;
-                    int st = 0;
-                    if (!ok || !isfinite(Fo)) st |= MM_ST_NONFINITE;
-                    if (valid) {
-                        P.F[gi] = Fo;
-                        if (P.R) P.R[gi] = Ro;
-                        if (P.status) P.status[gi] = st;
-                    }
-                }
-                __syncwarp();
-            } else {
-                // population matrix M' (rows i, columns j), right-hand side e_last
-                for (int i = 0; i < n_g; i++) {
-                    for (int j = t; j < n_g; j += G) {
-                        double a = (i == j) ? -Rk[j] : 0.0;
-                        for (int e = 0; e < n_e; e++) a = fma(Rm[j * LDR + e], BR[i * NEMAX + e], a);
-                        A[i * LDA + j] = (i == n_g - 1) ? 1.0 : a;
-                    }
-                }
-                for (int i = t; i < n_g; i += G) bv[i] = (i == n_g - 1) ? 1.0 : 0.0;
-                __syncwarp();
-                // elimination with partial pivoting
-                for (int col = 0; col < n_g; col++) {
-                    double best = -1.0;
-                    int brow = n_g;
-                    for (int r = col + t; r < n_g; r += G) {
-                        const double a = fabs(A[r * LDA + col]);
-                        if (a > best) { best = a; brow = r; }
-                    }
-                    for (int o = G >> 1; o > 0; o >>= 1) {
-                        const double ob = __shfl_xor_sync(0xffffffffu, best, o);
-                        const int orow = __shfl_xor_sync(0xffffffffu, brow, o);
-                        if (ob > best || (ob == best && orow < brow)) { best = ob; brow = orow; }
-                    }
-                    const int prow = brow;
-                    if (prow != col) {
-                        for (int j = t; j < n_g; j += G) {
-                            const double tmp = A[col * LDA + j];
-                            A[col * LDA + j] = A[prow * LDA + j];
-                            A[prow * LDA + j] = tmp;
-                        }
-                        if (t == 0) { const double tb = bv[col]; bv[col] = bv[prow]; bv[prow] = tb; }
-                    }
-                    __syncwarp();
-                    const double pv = A[col * LDA + col];
-                    const double ap = fabs(pv);
-                    const double y = mm_rcp(ap >= 1e-30 ? pv : 1.0);
-                    const double inv_e = (ap < 1e-30) ? 0.0 : y;
-                    if (ap < 1e-30) stat |= MM_ST_PIVOT;
-                    if (t == 0) invU[col] = (ap > 1e-30) ? y : 0.0;
-                    for (int r = col + 1 + t; r < n_g; r += G) A[r * LDA + col] *= inv_e;
-                    __syncwarp();
-                    for (int r = col + 1; r < n_g; r++) {
-                        const double f = A[r * LDA + col];
-                        for (int j = col + 1 + t; j < n_g; j += G)
-                            A[r * LDA + j] = fma(-f, A[col * LDA + j], A[r * LDA + j]);
-                    }
-                    for (int r = col + 1 + t; r < n_g; r += G)
-                        bv[r] = fma(-A[r * LDA + col], bv[col], bv[r]);
-                    __syncwarp();
-                }
-                // back substitution
-                for (int i = n_g - 1; i >= 0; i--) {
-                    double part = 0.0;
-                    for (int j = i + 1 + t; j < n_g; j += G) part = fma(A[i * LDA + j], xv[j], part);
-                    part = gsum(part, G);
-                    const double xi = (bv[i] - part) * invU[i];
-                    __syncwarp();
-                    if (t == 0) xv[i] = xi;
-                    __syncwarp();
-                }
-                // clamp, normalise, force
-                double tot = 0.0, Fs = 0.0, Rs = 0.0;
-                for (int i = t; i < n_g; i += G) {
-                    const double p = xv[i] > 0.0 ? xv[i] : 0.0;
-                    tot += p;
-                    Fs = fma(p, Fk[i], Fs);
-                    Rs = fma(p, Rk[i], Rs);
-                }
-                // uniform-population sums, reduced outside the branch (both 16-lane groups
-                // of a warp take every shuffle)
-                double fu = 0.0, ru = 0.0;
-                for (int i = t; i < n_g; i += G) { fu += Fk[i]; ru += Rk[i]; }
-                tot = gsum(tot, G);
-                Fs = gsum(Fs, G);
-                Rs = gsum(Rs, G);
-                fu = gsum(fu, G);
-                ru = gsum(ru, G);
-                double Fo, Ro;
-                if (tot > 0.0) {
-                    const double it = mm_rcp(tot);
-                    Fo = Fs * it;
-                    Ro = Rs * it;
-                } else {
-                    stat |= MM_ST_ZERO_POP;
-                    Fo = P.uniform_fb ? fu / n_g : 0.0;
-                    Ro = P.uniform_fb ? ru / n_g : 0.0;
-                }
-                if (!isfinite(Fo)) stat |= MM_ST_NONFINITE;
-                for (int o = G >> 1; o > 0; o >>= 1) stat |= __shfl_xor_sync(0xffffffffu, stat, o);
-                if (valid && t == 0) {
-                    P.F[gi] = Fo;
-                    if (P.R) P.R[gi] = Ro;
-                    if (P.status) P.status[gi] = stat;
-                }
+            const SmOut r = sm_point<NGMAX, NEMAX, G, RED>(M, Bm, W, t, P.v[gi], P.z[gi], Bm.Bg, P.geff,
+                                                           P.uniform_fb, nullptr);
+            if (valid && t == 0) {
+                P.F[gi] = r.F;
+                if (P.R) P.R[gi] = r.R;
+                if (P.status) P.status[gi] = r.status;
             }
         }
     }

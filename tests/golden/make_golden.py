@@ -281,10 +281,11 @@ def molecules_golden():
 def force3d_reference_golden():
     """The reference's 3D model (molmot/mot/simulator_3d.py:168-365
     rate_eq_force_3d, :443-504 MOTSimulator3D.simulate_trajectory_3d) run on
-    synthetic molecules whose ground Zeeman Hamiltonian has a non-degenerate
-    spectrum (molmot_b200.molecules.synthetic; the eigenbasis, and so the
-    force, is a well-posed function of the inputs): 72 (r, v) points and
-    3 leapfrog trajectories of 200 steps per molecule.  Also the reference's
+    synthetic molecules (12 + 4, 8 + 3 and 16 + 8 levels) whose ground Zeeman
+    Hamiltonian has a non-degenerate spectrum (molmot_b200.molecules.synthetic;
+    the eigenbasis, and so the force, is a well-posed function of the
+    inputs): 72 (r, v) points and 3 leapfrog trajectories of 200 steps per
+    molecule.  Also the reference's
     own spread on the SrOH cases of force3d_golden.npz: the largest change of
     its force under 1e-15 relative Hermitian perturbations of the Zeeman
     Hamiltonian passed to numpy.linalg.eigh (6 draws per case), relative to
@@ -295,7 +296,8 @@ def force3d_reference_golden():
     sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
     from molmot_b200.molecules.synthetic import synthetic_molecule
     out = {"versions": versions()}
-    mols = [(12, 4, 5, -0.5, 0.5, 1.0, 0.2), (8, 3, 21, -0.8, 0.3, 2.0, 0.25)]
+    mols = [(12, 4, 5, -0.5, 0.5, 1.0, 0.2), (8, 3, 21, -0.8, 0.3, 2.0, 0.25),
+            (16, 8, 41, -0.6, 0.4, 1.5, 0.22)]
     out["n_mol"] = len(mols)
     for i, (ng, ne, seed, d, sp, s0_, Bg) in enumerate(mols):
         m = synthetic_molecule(ng, ne, seed)

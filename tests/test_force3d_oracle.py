@@ -23,7 +23,7 @@ def _beams(g, i):
     return tuple(g[f"m{i}_{k}"] for k in ("khat", "freq", "q", "s0", "radius"))
 
 
-@pytest.mark.parametrize("i", [0, 1])
+@pytest.mark.parametrize("i", [0, 1, 2])
 def test_oracle_force3d_matches_reference(i):
     from oracle import force3d as o3
     g = golden("force3d_reference.npz")
@@ -40,7 +40,7 @@ def test_oracle_force3d_matches_reference(i):
     assert np.abs(P - g[f"m{i}_P"]).max() <= TOL
 
 
-@pytest.mark.parametrize("i", [0, 1])
+@pytest.mark.parametrize("i", [0, 1, 2])
 def test_oracle_leapfrog_matches_reference(i):
     from oracle import force3d as o3
     g = golden("force3d_reference.npz")

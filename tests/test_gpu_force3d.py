@@ -43,7 +43,7 @@ def synth(gpu):
     return m, sim, beams3
 
 
-@pytest.mark.parametrize("i", [0, 1])
+@pytest.mark.parametrize("i", [0, 1, 2])
 def test_force3d_synthetic_vs_reference(gpu, i):
     from molmot_b200.engine import beam_sets_3d, force3d_batch, pack_for
     from molmot_b200.molecules.synthetic import synthetic_molecule
@@ -58,7 +58,7 @@ def test_force3d_synthetic_vs_reference(gpu, i):
     assert np.abs(P - K("P")).max() <= TOL3D
 
 
-@pytest.mark.parametrize("i", [0, 1])
+@pytest.mark.parametrize("i", [0, 1, 2])
 def test_leapfrog_synthetic_vs_reference(gpu, i):
     from molmot_b200.molecules.synthetic import synthetic_molecule
     from molmot_b200.simulator_3d import MOTSimulator3D, make_beam_pairs_dc4
