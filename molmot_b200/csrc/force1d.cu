@@ -263,7 +263,7 @@ force_reduced_adjoint_kernel(ForceParams P, double *grad)
 {
     extern __shared__ __align__(16) unsigned char sm[];
     RedLayout<NGMAX, NEMAX> Ly;
-    Ly.build(P.n_b);
+    Ly.build(P.n_b, true);
     const long long pts_per_set = (P.layout == MM_LAYOUT_GRID) ? P.nv * P.nz : P.pps;
     const int nb = P.n_b, gw = 2 * nb + 1, st = blockDim.x;
     double *fd = (double *)(sm + Ly.total) + threadIdx.x;
@@ -532,7 +532,7 @@ traj_grad_kernel(ForceParams P, TgParams T)
 {
     extern __shared__ __align__(16) unsigned char sm[];
     RedLayout<NGMAX, NEMAX> Ly;
-    Ly.build(P.n_b);
+    Ly.build(P.n_b, true);
     RedView S;
     build_reduced_tables<NGMAX, NEMAX, PAD, true>(P, 0, sm, Ly, S);
     const int nb = P.n_b, st = blockDim.x, np = T.n_par, W = 6 + 6 * np;
@@ -765,7 +765,7 @@ int launch_reduced_adjoint(const ForceParams &P, double *grad, cudaStream_t st)
 {
     auto kern = force_reduced_adjoint_kernel<C::ng, C::ne, C::exact, PAD>;
     RedLayout<C::ng, C::ne> Ly;
-    Ly.build(P.n_b);
+    Ly.build(P.n_b, true);
     const size_t sb = Ly.total + sizeof(double) * 3 * P.n_b * kRedThreads;
     if (sb > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb);
@@ -791,7 +791,7 @@ int launch_traj_grad(const ForceParams &P, const TgParams &T, cudaStream_t st)
 {
     auto kern = traj_grad_kernel<C::ng, C::ne, C::exact, PAD>;
     RedLayout<C::ng, C::ne> Ly;
-    Ly.build(P.n_b);
+    Ly.build(P.n_b, true);
     const size_t sb = Ly.total + sizeof(double) * 3 * P.n_b * kTgThreads;
     if (sb > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb);

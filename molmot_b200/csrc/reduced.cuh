@@ -79,9 +79,10 @@ template <int NGMAX, int NEMAX>
 struct RedLayout {
     // offs[g*NEMAX + e] .. offs[g*NEMAX + e + 1]: triples of (g, e), beams ascending
     static constexpr int n_offs = NGMAX * NEMAX + 1;
-    size_t offs, brt, rsum, flags, E, czd, zde, freq, ck, trip, total;
+    size_t offs, brt, rsum, flags, E, czd, zde, freq, ck, trip, d2t, total;
     __host__ __device__ static size_t al(size_t x) { return (x + 15) & ~size_t(15); }
-    __host__ __device__ void build(int n_b)
+    // with_d2: also |d|^2 of every triple slot (the adjoints' d/ds0 terms)
+    __host__ __device__ void build(int n_b, bool with_d2 = false)
     {
         size_t o = 0;
         offs = o;  o = al(o + sizeof(int) * n_offs);
@@ -93,8 +94,10 @@ struct RedLayout {
         zde = o;   o = al(o + sizeof(double) * NEMAX);            // zd_e,
         freq = o;  o = al(o + sizeof(double) * n_b);              // beam frequencies,
         ck = o;    o = al(o + sizeof(double) * n_b);              // -k kdir_b
-        trip = o;  o = al(o + sizeof(TripR) * (size_t)NGMAX * NEMAX *
-                                  (size_t)((n_b + kRedPad - 1) / kRedPad * kRedPad));
+        const size_t slots = (size_t)NGMAX * NEMAX * (size_t)((n_b + kRedPad - 1) / kRedPad * kRedPad);
+        trip = o;  o = al(o + sizeof(TripR) * slots);
+        d2t = with_d2 ? o : 0;
+        if (with_d2) o = al(o + sizeof(double) * slots);
         total = o;
     }
 };
@@ -104,6 +107,7 @@ struct RedView {
     const double *brt, *rsum;
     const double *E, *czd, *zde, *freq, *ck;
     const void *trip;  // TripR (FP32 form) or TripD (FP64 form)
+    const double *d2t; // |d|^2 per triple slot (layouts built with_d2), else null
     int valid;
 };
 
@@ -189,6 +193,7 @@ __device__ void build_reduced_tables(const ForceParams &P, int set, unsigned cha
             const double d2 = P.d2[(g * n_e + e) * 3 + pol[b]];
             if (d2 < 1e-15) continue;
             if constexpr (F64) {  // the plain form's products, in its order
+                if (Ly.d2t) ((double *)(sm + Ly.d2t))[o] = d2;
                 TripD tr;
                 tr.c1 = __dmul_rn(__dmul_rn(gh, s0[b]), d2) * P.geff;
                 tr.c2 = __dmul_rn(s0[b], d2);
@@ -209,6 +214,7 @@ __device__ void build_reduced_tables(const ForceParams &P, int set, unsigned cha
         }
         for (; o < offs[i + 1]; o++) {  // zero-weight padding: every term 0
             if constexpr (F64) {
+                if (Ly.d2t) ((double *)(sm + Ly.d2t))[o] = 0.0;
                 TripD tr = {};
                 tr.pad = 1;  // marks list padding for the adjoint
                 tripd[o] = tr;
@@ -220,6 +226,7 @@ __device__ void build_reduced_tables(const ForceParams &P, int set, unsigned cha
     }
     __syncthreads();
     S.offs = offs; S.brt = brt; S.rsum = rsum; S.trip = trip; S.valid = flags[0];
+    S.d2t = Ly.d2t ? (const double *)(sm + Ly.d2t) : nullptr;
     S.E = Es; S.czd = czd; S.zde = zde; S.freq = frq; S.ck = ck;
 }
 
@@ -741,7 +748,7 @@ __device__ __forceinline__ RedOut reduced_adjoint_point(const ForceParams &P, co
                 const double q = fma(alpha + beta * tr.hk, tr.c1, gamma * tr.c2);
                 gf[b * stride] = fma(q * dLd, MM_TWO_PI, gf[b * stride]);
                 // d(c1, c2)/ds0_b with d2 = c2 / s0_b written out: c1 = ((Gamma/2) s0 d2) Geff
-                const double d2 = P.d2[(g * P.n_e + e) * 3 + pol[b]];
+                const double d2 = S.d2t[i];
                 const double qs = fma((alpha + beta * tr.hk) * gh * P.geff, d2, gamma * d2);
                 gs[b * stride] = fma(qs, L, gs[b * stride]);
                 gBG = fma(q * dLd, dBde, gBG);

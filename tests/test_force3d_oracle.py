@@ -65,3 +65,56 @@ def test_reference_sroh_spread_is_recorded():
     s = g["sroh_spread"]
     assert s.shape == (int(golden("force3d_golden.npz")["n_cases"]),)
     assert np.all(s > 1e-3)
+
+
+@pytest.mark.parametrize("i", [0, 2])
+def test_torch_restatement_matches_reference_and_fd(i):
+    """oracle/torch_dense3d.py (the autograd checker of the 3D tangents)
+    reproduces the reference's 3D force on the non-degenerate molecules, and
+    its autograd derivatives agree with central differences of the numpy
+    oracle (with respect to position, velocity, a beam frequency, a
+    saturation parameter and B')."""
+    import torch
+    from oracle import force3d as o3
+    from oracle import torch_dense3d as td3
+    g = golden("force3d_reference.npz")
+    m = _mol(g, i)
+    kh, fq, q, s0, rad = _beams(g, i)
+    B = float(g[f"m{i}_B"])
+    r = torch.tensor(g[f"m{i}_r"][:16], dtype=torch.float64)
+    v = torch.tensor(g[f"m{i}_v"][:16], dtype=torch.float64)
+    F, R, P = td3.force3d(m, kh, fq, q, s0, rad, r, v, B)
+    Fg = g[f"m{i}_F"][:16]
+    assert np.abs(F.numpy() - Fg).max() <= 1e-12 * np.abs(Fg).max()
+    # derivatives at one point
+    j = 3
+    rr = r[j:j + 1].clone().requires_grad_(True)
+    vv = v[j:j + 1].clone().requires_grad_(True)
+    fqt = torch.tensor(fq, requires_grad=True)
+    s0t = torch.tensor(s0, requires_grad=True)
+    Bt = torch.tensor(B, dtype=torch.float64, requires_grad=True)
+    Fz = td3.force3d(m, kh, fqt, q, s0t, rad, rr, vv, Bt)[0][0, 2]
+    gr, gv, gf, gs, gB = torch.autograd.grad(Fz, [rr, vv, fqt, s0t, Bt])
+    base = lambda **kw: o3.force3d(m, kw.get("kh", kh), kw.get("fq", fq), q, kw.get("s0", s0), rad,
+                                   kw.get("r", r[j].numpy()), kw.get("v", v[j].numpy()),
+                                   kw.get("B", B))[0][2]
+
+    def cd(key, x0, h, idx=None):
+        xp, xm = np.array(x0, dtype=float), np.array(x0, dtype=float)
+        if idx is None:
+            xp, xm = x0 + h, x0 - h
+        else:
+            xp[idx] += h
+            xm[idx] -= h
+        return (base(**{key: xp}) - base(**{key: xm})) / (2 * h)
+
+    # central differences carry ~1e-4 of truncation and rounding noise here (the
+    # transition frequencies round to 1/16 Hz at 4.3e14 Hz): 2e-3 relative
+    close = lambda fd, ad: abs(fd - ad) <= 2e-3 * abs(ad)
+    for c in range(3):
+        assert close(cd("r", r[j].numpy(), 1e-6, c), gr[0, c].item()), ("r", c)
+        assert close(cd("v", v[j].numpy(), 1e-3, c), gv[0, c].item()), ("v", c)
+    b = 2
+    assert close(cd("fq", fq, 2.0e4, b), gf[b].item())
+    assert close(cd("s0", s0, 1e-4 * s0[b], b), gs[b].item())
+    assert close(cd("B", B, 1e-4 * B), gB.item())
