@@ -277,6 +277,32 @@ def _ev_time(torch, fn, reps=3):
     return e0.elapsed_time(e1) / reps
 
 
+def _graph_time(torch, fn, reps=20):
+    """Device time of fn (ms) with the host's launch overhead taken out: fn is
+    captured once in a CUDA graph (outputs from the graph's own pool) and the
+    graph is replayed reps times between two events."""
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        fn()  # warm-up outside capture (kernel attributes, module load)
+    torch.cuda.current_stream().wait_stream(s)
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        fn()
+    g.replay()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        g.replay()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    del g
+    return ms
+
+
 def secondary_measurements(torch, mol, pack, dev, peaks):
     """Particle-steps/s of the trajectory ensembles and the adjoint's cost."""
     from molmot_b200.engine import BeamSets, force_batch, force_adjoint, traj
@@ -350,14 +376,16 @@ def secondary_measurements(torch, mol, pack, dev, peaks):
     vs = np.linspace(-0.1, 0.1, 33)
     v = torch.as_tensor(np.tile(np.concatenate([np.zeros(33), vs]), 1024), device=dev)
     z = torch.as_tensor(np.tile(np.concatenate([zs, np.zeros(33)]), 1024), device=dev)
-    tf = _ev_time(torch, lambda: force_batch(pack, bsa, v, z, points_per_set=66, want_pop=False,
-                                             want_R=False, want_status=False), 5)
-    ta = _ev_time(torch, lambda: force_adjoint(pack, bsa, v, z, points_per_set=66), 5)
-    trf = _ev_time(torch, lambda: force_batch(pack, bsa, v, z, points_per_set=66, want_pop=False,
-                                              want_R=False, want_status=False,
-                                              precision="fp64_reduced"), 5)
-    tra = _ev_time(torch, lambda: force_adjoint(pack, bsa, v, z, points_per_set=66,
-                                                precision="fp64_reduced"), 5)
+    # each form's kernels timed from CUDA-graph replays (these launches take ~0.1 ms,
+    # the size of the host's per-call overhead)
+    tf = _graph_time(torch, lambda: force_batch(pack, bsa, v, z, points_per_set=66, want_pop=False,
+                                                want_R=False, want_status=False))
+    ta = _graph_time(torch, lambda: force_adjoint(pack, bsa, v, z, points_per_set=66))
+    trf = _graph_time(torch, lambda: force_batch(pack, bsa, v, z, points_per_set=66, want_pop=False,
+                                                 want_R=False, want_status=False,
+                                                 precision="fp64_reduced"))
+    tra = _graph_time(torch, lambda: force_adjoint(pack, bsa, v, z, points_per_set=66,
+                                                   precision="fp64_reduced"))
     out["adjoint"] = {"workload": "1024 parameter sets x (33 z + 33 v) stencil points, gradients "
                                   "w.r.t. 8 beam frequencies, 8 s0 and B'",
                       "forward_ms": tf, "forward_plus_adjoint_ms": ta, "cost_ratio": ta / tf,

@@ -289,6 +289,53 @@ MM_API int mm_traj_grad_run(const mm_pack *pack, const mm_beams *beams, const mm
                             int64_t n_particles, double *state, int32_t *n_actual, double *ckpt,
                             void *stream);
 
+/* Options of mm_traj3d_grad_run. */
+typedef struct {
+    int64_t n_steps;     /* as mm_traj3d_run: step0 = 0 applies the first half kick and runs updates
+                            j = 1 .. n_steps - 1; step0 > 0 runs updates j = step0 .. step0 + n_steps - 1 */
+    int64_t step0;       /* absolute index of the first update (0 for a new run)                   */
+    int64_t ckpt_every;  /* with ckpt non-NULL: the state after every update j with j % ckpt_every == 0;
+                            resume from it with step0 = j + 1                                     */
+    double dt;           /* s                                                                     */
+    double r_escape;     /* m: |r| beyond which a particle stops                                  */
+    double hbar;         /* J s; <= 0 selects CODATA 1.054571817e-34 (the 3D reference's value)  */
+    double gap_tol;      /* relative ground Zeeman eigenvalue gap below which the eigenbasis
+                            derivative is undefined (status MM_ST_DEGENERATE); <= 0 selects 1e-9 */
+    uint64_t seed;       /* Philox key of the recoil kicks (mm_traj3d_run's)                      */
+    int32_t kicks;       /* != 0: recoil kicks, held fixed under differentiation                  */
+    int32_t n_par;       /* parameters theta_k, 1..MM_TGRAD_MAX_PAR                               */
+    int32_t freq_par[MM_MAX_BEAMS]; /* parameter whose value adds to beam b's frequency, or -1     */
+    int32_t s0_par[MM_MAX_BEAMS];   /* parameter whose value adds to beam b's s0, or -1            */
+    int32_t bprime_par;  /* parameter that adds to B', or -1                                      */
+    int32_t reserved;
+} mm_t3grad_opts;
+
+#define MM_ST_DEGENERATE 8 /* status bit of mm_traj3d_grad_run: a step met a degenerate ground
+                              Zeeman spectrum (gap below gap_tol), where d(force)/d(position)
+                              is not defined; the terms through that pair were dropped */
+
+/*
+ * The 3D leapfrog ensemble of mm_traj3d_run (MOTSimulator3D.simulate_trajectory_3d,
+ * molmot/mot/simulator_3d.py:443-504; beam set 0, its bits and recoil kicks) carried with
+ * its tangents d(r, v)/d theta_k (forward mode) through the 24-beam force, the field
+ * dependence of the ground Zeeman eigenbasis included (first-order perturbation theory of
+ * the eigenvectors, defined for a non-degenerate spectrum; the reference's SrOH spectrum is
+ * degenerate and is flagged).  No counterpart in the reference (new on this path).
+ * state [N][6 + 6 n_par] (in/out): r[3], v_half[3], dr[3][n_par], dv_half[3][n_par]; for
+ * step0 = 0 pass v0 and the initial tangents (zero for initial conditions that do not depend
+ * on theta) in place of v_half.  vsync [N][3 + 3 n_par] (out): the synchronised velocity of
+ * the last update and its tangent (mean kinetic energy gradients: m v . dv).  n_actual [N]
+ * (in/out; 0 for a new run), status [N] (out), n_events [N] (nullable).  ckpt
+ * [mm_traj3d_grad_checkpoints(step0, n_steps, ckpt_every)][N][6 + 6 n_par] (nullable).
+ * Molecules up to 16 ground and 8 excited states.
+ */
+MM_API int mm_traj3d_grad_run(const mm_pack *pack, const mm_beams *beams, const mm_t3grad_opts *opts,
+                              int64_t n_particles, double *state, double *vsync, int32_t *n_actual,
+                              int32_t *status, int32_t *n_events, double *ckpt, void *stream);
+
+/* Number of checkpoints one mm_traj3d_grad_run call writes. */
+MM_API int64_t mm_traj3d_grad_checkpoints(int64_t step0, int64_t n_steps, int64_t ckpt_every);
+
 /*
  * N independent 1D trajectories with symplectic Euler, one beam set (set 0).
  * Replaces traj_kernel / simulate_trajectories_cuda

@@ -23,6 +23,7 @@ MM_LAYOUT_GRID = 1
 MM_ST_PIVOT = 1
 MM_ST_NONFINITE = 2
 MM_ST_ZERO_POP = 4
+MM_ST_DEGENERATE = 8
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int32)
@@ -64,6 +65,15 @@ class TgradOpts(ctypes.Structure):
     _fields_ = [("n_steps", ctypes.c_int64), ("step0", ctypes.c_int64),
                 ("ckpt_every", ctypes.c_int64), ("dt", ctypes.c_double),
                 ("r_escape", ctypes.c_double), ("hbar", ctypes.c_double),
+                ("seed", ctypes.c_uint64), ("kicks", ctypes.c_int32), ("n_par", ctypes.c_int32),
+                ("freq_par", ctypes.c_int32 * MM_MAX_BEAMS), ("s0_par", ctypes.c_int32 * MM_MAX_BEAMS),
+                ("bprime_par", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+
+
+class T3gradOpts(ctypes.Structure):
+    _fields_ = [("n_steps", ctypes.c_int64), ("step0", ctypes.c_int64),
+                ("ckpt_every", ctypes.c_int64), ("dt", ctypes.c_double),
+                ("r_escape", ctypes.c_double), ("hbar", ctypes.c_double), ("gap_tol", ctypes.c_double),
                 ("seed", ctypes.c_uint64), ("kicks", ctypes.c_int32), ("n_par", ctypes.c_int32),
                 ("freq_par", ctypes.c_int32 * MM_MAX_BEAMS), ("s0_par", ctypes.c_int32 * MM_MAX_BEAMS),
                 ("bprime_par", ctypes.c_int32), ("reserved", ctypes.c_int32)]
@@ -111,6 +121,9 @@ SIGNATURES = {
                                          ctypes.c_double, _vp, _vp]),
     "mm_histogram": (ctypes.c_int, [_vp, ctypes.c_int64, ctypes.c_int64, ctypes.c_double, ctypes.c_double,
                                     ctypes.c_int32, _vp, _vp]),
+    "mm_traj3d_grad_run": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(T3gradOpts), ctypes.c_int64, _vp, _vp,
+                                          _vp, _vp, _vp, _vp, _vp]),
+    "mm_traj3d_grad_checkpoints": (ctypes.c_int64, [ctypes.c_int64, ctypes.c_int64, ctypes.c_int64]),
     "mm_traj_grad_run": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(TgradOpts), ctypes.c_int64, _vp, _vp,
                                         _vp, _vp]),
 }

@@ -149,6 +149,17 @@ struct Out3 {
     int status;
 };
 
+// Lane-local values of one point kept for the tangent pass (lane t = sorted
+// ground eigenstate t): unsaturated and saturated rates per excited state,
+// the saturation sum and factor, the unsaturated force vector, the total rate,
+// the population before the clamp, the population and the population sum.
+template <int NGM, int NEM>
+struct Keep3 {
+    double Ru[NEM], Rs[NEM], sg, cg, Fv[3], Rk, xraw, x, tot;
+    double A[NGM], invd;  // this lane's column of the eliminated population matrix, 1/pivot
+    int prow[NGM];        // row interchanges of the elimination (same on every lane)
+};
+
 
 // One round of NGM/2 disjoint complex Jacobi rotations (H <- J^H H J,
 // V <- V J, J = [[c, s], [-conj(s), c]] on columns p, q).  pq[i] holds the
@@ -232,7 +243,8 @@ __device__ __forceinline__ void jacobi_round(GroupT &W, int t, const unsigned sh
 template <int NGM, int NEM, int TH>
 __device__ Out3 force3d_point(const Force3Params &P, Smem3<NGM, NEM, TH> &S,
                               typename Smem3<NGM, NEM, TH>::Group &W, int t, int gbase,
-                              const double r[3], const double v[3], double Bg, double &pl)
+                              const double r[3], const double v[3], double Bg, double &pl,
+                              Keep3<NGM, NEM> *kp = nullptr)
 {
     constexpr int LDH = NGM + 1;
     constexpr unsigned FULL = 0xffffffffu;
@@ -394,9 +406,21 @@ __device__ Out3 force3d_point(const Force3Params &P, Smem3<NGM, NEM, TH> &S,
         }
     }
     const double cg = gh * P.geff * mm_rcp(1.0 + sg);  // rate = cg * unsaturated sum
+    if (kp) {
+#pragma unroll
+        for (int e = 0; e < NEM; e++) kp->Ru[e] = Racc[e];
+        kp->sg = sg;
+        kp->cg = cg;
+        for (int c = 0; c < 3; c++) kp->Fv[c] = Fv[c];
+    }
     double Rk = 0.0;
 #pragma unroll
     for (int e = 0; e < NEM; e++) { Racc[e] *= cg; Rk += Racc[e]; }
+    if (kp) {
+#pragma unroll
+        for (int e = 0; e < NEM; e++) kp->Rs[e] = Racc[e];
+        kp->Rk = Rk;
+    }
 
     // 5. population matrix (lane k owns column k), elimination, back substitution
     double A[NGM], bv[NGM];
@@ -427,6 +451,7 @@ __device__ Out3 force3d_point(const Force3Params &P, Smem3<NGM, NEM, TH> &S,
                     if (rr < n_g && fabs(A[rr]) > mx) { mx = fabs(A[rr]); prow = rr; }
             }
             prow = __shfl_sync(FULL, prow, gbase + col);
+            if (kp) kp->prow[col] = prow;
             if (__any_sync(FULL, prow != col)) {
 #pragma unroll
                 for (int rr = col + 1; rr < NGM; rr++)
@@ -463,6 +488,12 @@ __device__ Out3 force3d_point(const Force3Params &P, Smem3<NGM, NEM, TH> &S,
             if (t == i) x = (bv[i] - part) * invd;
         }
     }
+    if (kp) {
+        kp->xraw = (t < n_g) ? x : 0.0;
+#pragma unroll
+        for (int i = 0; i < NGM; i++) kp->A[i] = A[i];
+        kp->invd = invd;
+    }
     if (t >= n_g || x < 0.0) x = 0.0;
     const double tot = gsum16(x);
     if (tot > 0.0) x *= mm_rcp(tot);
@@ -471,6 +502,7 @@ __device__ Out3 force3d_point(const Force3Params &P, Smem3<NGM, NEM, TH> &S,
         if (P.uniform_fb) x = (t < n_g) ? 1.0 / n_g : 0.0;
     }
     pl = x;
+    if (kp) { kp->x = x; kp->tot = tot; }
     // 6. force and scattering rate
     const double hk = P.hbar * P.k;
     Out3 o;
@@ -605,6 +637,457 @@ traj3d_kernel(Force3Params P, Traj3Params T)
     }
 }
 
+// ---------------------------------------------------------------------------
+// Trajectory tangents of the 3D leapfrog (forward mode): d(r, v)/d theta_k for
+// parameters theta_k that add to beam frequencies (freq_par), saturation
+// parameters (s0_par) and B' (bprime_par), through the 24-beam force
+// including the field dependence of the ground Zeeman eigenbasis.  With H =
+// B.Zh (Zh = Hermitian part of the Zeeman blocks) and a non-degenerate
+// spectrum, first-order perturbation theory gives, in the sorted eigenbasis,
+//   d lambda_a = Re Y[a][a],   d x_{a,j} = sum_{b != a} conj(Y[b][a]) / (lambda_a - lambda_b) x_{b,j},
+// Y = V^H dH V, x_{a,j} = v_a^H |tdm_j| (j = (e, q)); |x|^2 and the branching
+// ratios follow.  The rates, saturation, population solve (the forward's own
+// LU factors, M dx = -dM x) and the force are differentiated term by term.
+// A gap |lambda_a - lambda_b| below gap_tol max|lambda| makes the eigenbasis
+// (and dF/dr) undefined: the step's terms through that pair are dropped and
+// the particle's status gets MM_ST_DEGENERATE.
+
+struct Tg3Params {
+    double dt, r_escape, mass, v_rec, gap_tol;
+    long long n_particles, n_steps, step0, ckpt_every;
+    int n_par, kicks, bprime_par;
+    unsigned long long seed;
+    signed char freq_par[NBM], s0_par[NBM];
+    double *state;      // [N][6 + 6 n_par]: r, vh, dr[3][n_par], dvh[3][n_par] (in/out)
+    double *vsync;      // [N][3 + 3 n_par]: synchronised velocity and its tangent (out)
+    int32_t *n_actual;  // [N] in/out
+    int32_t *status;    // [N] out
+    int32_t *n_events;  // [N] out or null
+    double *ckpt;       // [n_steps / ckpt_every][N][6 + 6 n_par] or null
+};
+
+constexpr int kT3MaxPar = MM_TGRAD_MAX_PAR;
+constexpr int kT3Threads = 64;  // 4 particles per CTA (the tangent workspace is large)
+
+// Per-group workspace of the tangent pass.
+template <int NGM, int NEM>
+struct Tan3Work {
+    double Yre[NGM][3][NGM], Yim[NGM][3][NGM];  // lane a: column a of V^H Zh_c V (sorted basis)
+    double xr[NGM][NEM * 3], xi[NGM][NEM * 3];  // x_{a, e*3+q}
+    double LU[NGM][NGM];                         // the forward's factors, row i, column j
+    double invd[NGM];
+    double dBR[NEM][NGM];
+    double dbm[NBM][5];                          // per beam: d doppler, d s_eff, d w0..w2
+    double dr[kT3MaxPar][3], dv[kT3MaxPar][3];   // the direction of each parameter's tangent
+    double dF[kT3MaxPar][3];
+    double Tr[3][kT3MaxPar], Tv[3][kT3MaxPar], Tvs[3][kT3MaxPar];
+    double pad_[2];
+};
+
+// dF/d theta_k (k < n_par) at (r, v) along the directions TW.dr[k], TW.dv[k]
+// (the tangents of the force's position and velocity arguments), written to
+// TW.dF[k] by lane 0.  Runs after force3d_point(..., kp) on the same point
+// (its shared tables W and lane values kp).  Every lane of the warp calls it.
+template <int NGM, int NEM, int TH>
+__device__ void force3d_tangent(const Force3Params &P, const Tg3Params &T, Smem3<NGM, NEM, TH> &S,
+                                typename Smem3<NGM, NEM, TH>::Group &W, Tan3Work<NGM, NEM> &TW, int t,
+                                const double r[3], const double v[3], double Bg,
+                                const Keep3<NGM, NEM> &kp, int &stat)
+{
+    constexpr int LDH = NGM + 1;
+    const int n_g = P.n_g, n_e = P.n_e, n_b = P.n_b;
+    const double G = P.Gamma, gh = G / 2.0, gh2 = gh * gh;
+    const bool lane = t < n_g;
+    const int ca = lane ? W.perm[t] : 0;
+    // field and its direction
+    const double Bd[3] = {((-r[0]) / 2.0) * 1e4, ((-r[1]) / 2.0) * 1e4, r[2] * 1e4};  // dB/dB'
+    const double B[3] = {Bg * Bd[0], Bg * Bd[1], Bg * Bd[2]};
+    const double Bm = sqrt(B[0] * B[0] + B[1] * B[1] + B[2] * B[2]);
+    const double bh2 = (Bm > 1e-10) ? B[2] / Bm : 1.0;
+    const double ct = fmin(fmax(bh2, -1.0), 1.0);
+    // 1. x_{a,j} and column a of Y_c = V^H Zh_c V, once per point
+    if (lane) {
+        for (int e = 0; e < n_e; e++)
+            for (int q = 0; q < 3; q++) {
+                double ar = 0.0, ai = 0.0;
+                for (int g = 0; g < n_g; g++) {
+                    const double d = S.tdm[(g * n_e + e) * 3 + q];
+                    ar += W.Vre[g * LDH + ca] * d;
+                    ai -= W.Vim[g * LDH + ca] * d;
+                }
+                TW.xr[t][e * 3 + q] = ar;
+                TW.xi[t][e * 3 + q] = ai;
+            }
+        for (int c = 0; c < 3; c++) {
+            double wr[NGM], wi[NGM];
+#pragma unroll
+            for (int g = 0; g < NGM; g++) {
+                double ar = 0.0, ai = 0.0;
+                if (g < n_g) {
+                    for (int h = 0; h < n_g; h++) {
+                        // Zh[g][h] = (Z[g][h] + conj(Z[h][g])) / 2
+                        const double zr = 0.5 * (S.Zre[c][g * n_g + h] + S.Zre[c][h * n_g + g]);
+                        const double zi = 0.5 * (S.Zim[c][g * n_g + h] - S.Zim[c][h * n_g + g]);
+                        const double vr = W.Vre[h * LDH + ca], vi = W.Vim[h * LDH + ca];
+                        ar += zr * vr - zi * vi;
+                        ai += zr * vi + zi * vr;
+                    }
+                }
+                wr[g] = ar;
+                wi[g] = ai;
+            }
+            for (int b = 0; b < n_g; b++) {
+                const int cb = W.perm[b];
+                double yr = 0.0, yi = 0.0;
+#pragma unroll
+                for (int g = 0; g < NGM; g++) {
+                    if (g < n_g) {  // conj(V[g][cb]) w[g]
+                        const double vr = W.Vre[g * LDH + cb], vi = W.Vim[g * LDH + cb];
+                        yr += vr * wr[g] + vi * wi[g];
+                        yi += vr * wi[g] - vi * wr[g];
+                    }
+                }
+                TW.Yre[t][c][b] = yr;
+                TW.Yim[t][c][b] = yi;
+            }
+        }
+        // the forward's population factors, column t
+        for (int i = 0; i < n_g; i++) TW.LU[i][t] = kp.A[i];
+        TW.invd[t] = kp.invd;
+    }
+    __syncwarp();
+    double lmax = 0.0;
+    for (int a = 0; a < n_g; a++) lmax = fmax(lmax, fabs(W.lam[a]));
+    const double gap_min = T.gap_tol * lmax;
+    // excited-state totals of |x|^2 (the branching ratios' denominators)
+    double tot_e[NEM];
+#pragma unroll
+    for (int e = 0; e < NEM; e++) {
+        double a = 0.0;
+        if (e < n_e && lane)
+            for (int q = 0; q < 3; q++) a += W.dsq[(e * 3 + q) * NGM + t];
+        tot_e[e] = gsum16(a);
+    }
+    const double hk = P.hbar * P.k;
+    for (int k = 0; k < T.n_par; k++) {
+        const double *dr = TW.dr[k], *dv = TW.dv[k];
+        const double dBg = (k == T.bprime_par) ? 1.0 : 0.0;
+        const double dB[3] = {dBg * Bd[0] + Bg * (((-dr[0]) / 2.0) * 1e4), dBg * Bd[1] + Bg * (((-dr[1]) / 2.0) * 1e4),
+                              dBg * Bd[2] + Bg * (dr[2] * 1e4)};
+        double dct = 0.0;
+        if (Bm > 1e-10 && bh2 > -1.0 && bh2 < 1.0) {
+            const double dBm = (B[0] * dB[0] + B[1] * dB[1] + B[2] * dB[2]) / Bm;
+            dct = (dB[2] - bh2 * dBm) / Bm;
+        }
+        // 2. eigenvalue and |x|^2 tangents of lane a = t
+        double dlam = 0.0, ddsq[NEM * 3];
+#pragma unroll
+        for (int j = 0; j < NEM * 3; j++) ddsq[j] = 0.0;
+        if (lane) {
+            dlam = dB[0] * TW.Yre[t][0][t] + dB[1] * TW.Yre[t][1][t] + dB[2] * TW.Yre[t][2][t];
+            double dxr[NEM * 3], dxi[NEM * 3];
+#pragma unroll
+            for (int j = 0; j < NEM * 3; j++) { dxr[j] = 0.0; dxi[j] = 0.0; }
+            for (int b = 0; b < n_g; b++) {
+                if (b == t) continue;
+                const double gap = W.lam[t] - W.lam[b];
+                if (!(fabs(gap) > gap_min)) { stat |= MM_ST_DEGENERATE; continue; }
+                const double ig = 1.0 / gap;
+                // conj(Y_k[b][a]) / gap
+                const double yr = (dB[0] * TW.Yre[t][0][b] + dB[1] * TW.Yre[t][1][b] + dB[2] * TW.Yre[t][2][b]) * ig;
+                const double yi = -(dB[0] * TW.Yim[t][0][b] + dB[1] * TW.Yim[t][1][b] + dB[2] * TW.Yim[t][2][b]) * ig;
+#pragma unroll
+                for (int j = 0; j < NEM * 3; j++) {
+                    if (j < n_e * 3) {
+                        const double xr = TW.xr[b][j], xi = TW.xi[b][j];
+                        dxr[j] += yr * xr - yi * xi;
+                        dxi[j] += yr * xi + yi * xr;
+                    }
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < NEM * 3; j++)
+                if (j < n_e * 3) ddsq[j] = 2.0 * (TW.xr[t][j] * dxr[j] + TW.xi[t][j] * dxi[j]);
+        }
+        // branching-ratio tangents dBR[e][a] = (d row_ea - BR[e][a] d tot_e) / tot_e
+#pragma unroll
+        for (int e = 0; e < NEM; e++) {
+            double drow = 0.0;
+            if (e < n_e && lane) drow = ddsq[e * 3] + ddsq[e * 3 + 1] + ddsq[e * 3 + 2];
+            const double dtot = gsum16(drow);
+            if (e < n_e && lane)
+                TW.dBR[e][t] = tot_e[e] > 1e-30 ? (drow - W.BR[e * n_g + t] * dtot) / tot_e[e] : 0.0;
+        }
+        // 3. per-beam tangents: doppler, Gaussian profile, polarisation weights
+        for (int b = t; b < n_b; b += kG3) {
+            const double *kh = S.khat[b];
+            TW.dbm[b][0] = -P.k * (kh[0] * dv[0] + kh[1] * dv[1] + kh[2] * dv[2]) / MM_TWO_PI;
+            double gf = 1.0, dgf = 0.0;
+            if (S.radius[b] > 0.0) {
+                const double rp = r[0] * kh[0] + r[1] * kh[1] + r[2] * kh[2];
+                const double rps0 = (r[0] * r[0] + r[1] * r[1] + r[2] * r[2]) - rp * rp;
+                const double w2 = S.radius[b] * S.radius[b];
+                gf = exp(-2.0 * fmax(rps0, 0.0) / w2);
+                if (rps0 > 0.0) {
+                    const double drp = dr[0] * kh[0] + dr[1] * kh[1] + dr[2] * kh[2];
+                    const double drps = 2.0 * (r[0] * dr[0] + r[1] * dr[1] + r[2] * dr[2]) - 2.0 * rp * drp;
+                    dgf = gf * (-2.0 / w2) * drps;
+                }
+            }
+            const double ds0 = (T.s0_par[b] == k) ? 1.0 : 0.0;
+            TW.dbm[b][1] = ds0 * gf + S.s0[b] * dgf;
+            const double dd = 0.5 * (1.0 + ct) * dct, dm = -ct * dct, dov = -0.5 * (1.0 - ct) * dct,
+                         dc = 2.0 * ct * dct;
+            const int q = S.pol[b];
+            double w0, w1, w2;
+            if (q == 0) { w0 = dd; w1 = dm; w2 = dov; }
+            else if (q == 1) { w0 = dm; w1 = dc; w2 = dm; }
+            else { w0 = dov; w1 = dm; w2 = dd; }
+            TW.dbm[b][2] = w0; TW.dbm[b][3] = w1; TW.dbm[b][4] = w2;
+        }
+        __syncwarp();
+        // 4. rate tangents of lane a = t (the forward's rate loop, differentiated)
+        double dRu[NEM], dFv[3] = {0.0, 0.0, 0.0}, dsg = 0.0;
+#pragma unroll
+        for (int e = 0; e < NEM; e++) dRu[e] = 0.0;
+        if (lane) {
+            const double Eg = W.Esg[t], dEg = dlam * G / (2 * MM_PI);
+            for (int b = 0; b < n_b; b++) {
+                const double fd = __dadd_rn(S.freq[b], W.bm[b][0]);
+                const double se = W.bm[b][1];
+                const double dfd = ((T.freq_par[b] == k) ? 1.0 : 0.0) + TW.dbm[b][0];
+                const double dse = TW.dbm[b][1];
+                double dQ = 0.0;
+#pragma unroll
+                for (int e = 0; e < NEM; e++) {
+                    if (e < n_e) {
+                        const double om = __dsub_rn(W.Ese[e], Eg);
+                        const double de = __dmul_rn(__dsub_rn(fd, om), MM_TWO_PI);
+                        const double L = gh2 * mm_rcp(fma(de, de, gh2));
+                        const double dEe = dB[2] * S.Ze[e] * G / MM_TWO_PI;
+                        const double dde = (dfd - (dEe - dEg)) * MM_TWO_PI;
+                        const double dL = -2.0 * de * L * L / gh2 * dde;
+                        double ws = 0.0, dws = 0.0;
+#pragma unroll
+                        for (int q = 0; q < 3; q++) {
+                            const double d2 = W.dsq[(e * 3 + q) * NGM + t];
+                            if (d2 >= 1e-15) {
+                                ws = fma(W.bm[b][2 + q], d2, ws);
+                                dws += TW.dbm[b][2 + q] * d2 + W.bm[b][2 + q] * ddsq[e * 3 + q];
+                            }
+                        }
+                        const double drb = (dws * L + ws * dL) * se + ws * L * dse;
+                        dRu[e] += drb;
+                        dQ += drb;
+                    }
+                }
+                dsg += dQ;
+                dFv[0] = fma(S.khat[b][0], dQ, dFv[0]);
+                dFv[1] = fma(S.khat[b][1], dQ, dFv[1]);
+                dFv[2] = fma(S.khat[b][2], dQ, dFv[2]);
+            }
+        }
+        const double dcg = -kp.cg * dsg / (1.0 + kp.sg);
+        double dRs[NEM], dRk = 0.0;
+#pragma unroll
+        for (int e = 0; e < NEM; e++) { dRs[e] = dRu[e] * kp.cg + kp.Ru[e] * dcg; dRk += dRs[e]; }
+        __syncwarp();
+        // 5. population tangent: M dx = -dM x (column t of dM on lane t; row n_g - 1 is constant)
+        double rhs[NGM];
+#pragma unroll
+        for (int i = 0; i < NGM; i++) {
+            double c = 0.0;
+            if (lane && i < n_g - 1) {
+                double a = (i == t) ? -dRk : 0.0;
+#pragma unroll
+                for (int e = 0; e < NEM; e++)
+                    if (e < n_e) a += dRs[e] * W.BR[e * n_g + i] + kp.Rs[e] * TW.dBR[e][i];
+                c = a * kp.xraw;
+            }
+            rhs[i] = -gsum16(c);
+        }
+        // P M = L U with the forward's interchanges and factors (later interchanges
+        // were applied to the stored L columns, so all of P goes first)
+#pragma unroll
+        for (int col = 0; col < NGM; col++) {
+            if (col < n_g) {
+                const int pr = kp.prow[col];
+#pragma unroll
+                for (int rr = col + 1; rr < NGM; rr++)
+                    if (rr == pr) { const double x = rhs[col]; rhs[col] = rhs[rr]; rhs[rr] = x; }
+            }
+        }
+#pragma unroll
+        for (int col = 0; col < NGM; col++) {
+            if (col < n_g) {
+                const double iv = TW.invd[col];
+#pragma unroll
+                for (int rr = col + 1; rr < NGM; rr++)
+                    if (rr < n_g) rhs[rr] = fma(-(TW.LU[rr][col] * iv), rhs[col], rhs[rr]);
+            }
+        }
+        double dx = 0.0, xs[NGM];
+#pragma unroll
+        for (int i = NGM - 1; i >= 0; i--) {
+            double xi = 0.0;
+            if (i < n_g) {
+                double part = 0.0;
+#pragma unroll
+                for (int j = i + 1; j < NGM; j++)
+                    if (j < n_g) part = fma(TW.LU[i][j], xs[j], part);
+                xi = (rhs[i] - part) * TW.invd[i];
+            }
+            xs[i] = xi;
+            if (i == t) dx = xi;
+        }
+        // clamp and normalisation
+        double dxc = (lane && kp.xraw > 0.0) ? dx : 0.0;
+        const double dtot = gsum16(dxc);
+        const double dp = (kp.tot > 0.0 && lane) ? (dxc - kp.x * dtot) / kp.tot : 0.0;
+        // 6. force tangent: F = hbar k sum_a p_a cg_a Fv_a
+        double f[3];
+        for (int c = 0; c < 3; c++) {
+            const double a = lane ? (dp * kp.cg * kp.Fv[c] + kp.x * (dcg * kp.Fv[c] + kp.cg * dFv[c])) : 0.0;
+            f[c] = hk * gsum16(a);
+        }
+        if (t == 0)
+            for (int c = 0; c < 3; c++) TW.dF[k][c] = f[c];
+        __syncwarp();
+    }
+}
+
+// Leapfrog ensemble with tangents, one particle per group: the trajectory of
+// traj3d_kernel (bit for bit, kicks included) plus d(r, vh, v)/d theta_k.
+template <int NGM, int NEM, int TH>
+__global__ void __launch_bounds__(TH)
+traj3d_grad_kernel(Force3Params P, Tg3Params T)
+{
+    extern __shared__ __align__(16) unsigned char smraw[];
+    auto &S = *reinterpret_cast<Smem3<NGM, NEM, TH> *>(smraw);
+    const int lane = threadIdx.x & 31, t = lane % kG3, gbase = lane - t;
+    const int group = threadIdx.x / kG3, ngroups = TH / kG3;
+    auto &TW = reinterpret_cast<Tan3Work<NGM, NEM> *>(smraw + (sizeof(Smem3<NGM, NEM, TH>) + 15) / 16 * 16)[group];
+    load_consts3(P, 0, S);
+    __syncthreads();
+    const double Bg = P.bgrad[0];
+    const double m = P.mass, dt = T.dt;
+    const int np = T.n_par, Wd = 6 + 6 * np;
+    const long long ip = (long long)blockIdx.x * ngroups + group;
+    const bool valid = ip < T.n_particles;
+    const long long ipc = valid ? ip : 0;
+    double *row = T.state + ipc * Wd;
+    double r[3], vh[3], vs[3], pl;
+    for (int c = 0; c < 3; c++) { r[c] = row[c]; vh[c] = row[3 + c]; vs[c] = vh[c]; }
+    for (int i = t; i < 3 * kT3MaxPar; i += kG3) {
+        const int c = i / kT3MaxPar, k = i % kT3MaxPar;
+        TW.Tr[c][k] = (k < np) ? row[6 + c * np + k] : 0.0;
+        TW.Tv[c][k] = (k < np) ? row[6 + 3 * np + c * np + k] : 0.0;
+        TW.Tvs[c][k] = TW.Tv[c][k];
+    }
+    __syncwarp();
+    int stat = 0, nev = 0;
+    Keep3<NGM, NEM> kp;
+    // a particle already beyond r_escape stopped in an earlier call
+    const bool stopped = !valid || sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]) > T.r_escape;
+    bool done = stopped;
+    long long na = -1, n_ck = 0;
+    auto set_dirs = [&]() {  // the force's argument tangents: TW.dr = Tr, TW.dv = Tv
+        for (int i = t; i < 3 * kT3MaxPar; i += kG3) {
+            const int c = i % 3, k = i / 3;
+            TW.dr[k][c] = TW.Tr[c][k];
+            TW.dv[k][c] = TW.Tv[c][k];
+        }
+        __syncwarp();
+    };
+    auto write_state = [&](double *dst) {
+        if (valid && t == 0) {
+            for (int c = 0; c < 3; c++) { dst[c] = r[c]; dst[3 + c] = vh[c]; }
+            for (int c = 0; c < 3; c++)
+                for (int k = 0; k < np; k++) {
+                    dst[6 + c * np + k] = TW.Tr[c][k];
+                    dst[6 + 3 * np + c * np + k] = TW.Tv[c][k];
+                }
+        }
+    };
+    if (T.step0 == 0) {  // first half kick at (r0, v0), as traj3d_kernel
+        set_dirs();
+        const Out3 o = force3d_point(P, S, S.grp[group], t, gbase, r, vh, Bg, pl, &kp);
+        force3d_tangent(P, T, S, S.grp[group], TW, t, r, vh, Bg, kp, stat);
+        for (int c = 0; c < 3; c++) vh[c] = vh[c] + 0.5 * dt * o.F[c] / m;
+        if (t < 3)
+            for (int k = 0; k < np; k++) TW.Tv[t][k] = fma(0.5 * dt / m, TW.dF[k][t], TW.Tv[t][k]);
+        __syncwarp();
+    }
+    const long long j0 = (T.step0 == 0) ? 1 : T.step0;
+    const long long j1 = T.step0 + T.n_steps;
+    long long j = j0;
+    for (; j < j1; j++) {
+        if (__all_sync(0xffffffffu, done)) break;
+        double rn[3];
+        for (int c = 0; c < 3; c++) rn[c] = __dadd_rn(r[c], __dmul_rn(dt, vh[c]));  // r + dt v_half
+        const double rr = sqrt(rn[0] * rn[0] + rn[1] * rn[1] + rn[2] * rn[2]);
+        const bool esc = !done && rr > T.r_escape;
+        // position tangent first: the force is evaluated at (r_j, v_half)
+        if (!done && t < 3)
+            for (int k = 0; k < np; k++) TW.Tr[t][k] = fma(dt, TW.Tv[t][k], TW.Tr[t][k]);
+        __syncwarp();
+        set_dirs();
+        const Out3 o = force3d_point(P, S, S.grp[group], t, gbase, rn, vh, Bg, pl, &kp);
+        int st = 0;
+        force3d_tangent(P, T, S, S.grp[group], TW, t, rn, vh, Bg, kp, st);
+        if (!done) {
+            stat |= st;
+            for (int c = 0; c < 3; c++) r[c] = rn[c];
+            if (esc) {
+                na = j;
+                done = true;
+                for (int c = 0; c < 3; c++) vs[c] = vh[c];
+                if (t < 3)
+                    for (int k = 0; k < np; k++) TW.Tvs[t][k] = TW.Tv[t][k];
+            } else {
+                double vn[3];
+                for (int c = 0; c < 3; c++) vn[c] = vh[c] + dt * o.F[c] / m;
+                if (T.kicks) {
+                    double kick[3];
+                    nev += recoil_kick(T.seed, (unsigned)ip, (unsigned)j, o.R * dt, T.v_rec, kick);
+                    for (int c = 0; c < 3; c++) vn[c] += kick[c];
+                }
+                for (int c = 0; c < 3; c++) { vs[c] = 0.5 * (vh[c] + vn[c]); vh[c] = vn[c]; }
+                if (t < 3)
+                    for (int k = 0; k < np; k++) {
+                        const double tvn = fma(dt / m, TW.dF[k][t], TW.Tv[t][k]);
+                        TW.Tvs[t][k] = 0.5 * (TW.Tv[t][k] + tvn);
+                        TW.Tv[t][k] = tvn;
+                    }
+            }
+        }
+        __syncwarp();
+        if (T.ckpt && j % T.ckpt_every == 0) {
+            write_state(T.ckpt + ((size_t)n_ck * T.n_particles + ipc) * Wd);
+            n_ck++;
+        }
+    }
+    // checkpoints after the whole warp stopped: the frozen state
+    if (T.ckpt)
+        for (; j < j1; j++)
+            if (j % T.ckpt_every == 0) {
+                write_state(T.ckpt + ((size_t)n_ck * T.n_particles + ipc) * Wd);
+                n_ck++;
+            }
+    write_state(row);
+    if (valid && t == 0) {
+        double *vo = T.vsync + ipc * (3 + 3 * np);
+        for (int c = 0; c < 3; c++) {
+            vo[c] = vs[c];
+            for (int k = 0; k < np; k++) vo[3 + c * np + k] = TW.Tvs[c][k];
+        }
+        if (na >= 0) T.n_actual[ip] = (int32_t)na;
+        else if (!stopped) T.n_actual[ip] = (int32_t)j1;
+        T.status[ip] = stat;
+        if (T.n_events) T.n_events[ip] = nev;
+    }
+}
+
 int fill3(const mm_pack *pack, const mm_beams *beams, double hbar, int uniform_fb, Force3Params &P)
 {
     if (!pack || !beams) { mm_set_error("null pack or beams handle"); return -1; }
@@ -732,4 +1215,97 @@ extern "C" int mm_traj3d_run(const mm_pack *pack, const mm_beams *beams, const d
     return dispatch3(P.n_g, P.n_e, [&](auto C) -> int {
         return launch_traj3d<decltype(C)>(P, T, (cudaStream_t)stream);
     });
+}
+
+namespace {
+
+// Checkpoints of one mm_traj3d_grad_run call: updates j in [j0, j1) with j % every == 0.
+long long t3_checkpoints(long long step0, long long n_steps, long long every)
+{
+    const long long j0 = (step0 == 0) ? 1 : step0, j1 = step0 + n_steps;
+    if (every < 1 || j1 <= j0) return 0;
+    return (j1 - 1) / every - (j0 - 1) / every;
+}
+
+template <class C>
+int launch_traj3d_grad(const Force3Params &P, const Tg3Params &T, cudaStream_t st)
+{
+    constexpr int TH = kT3Threads;
+    auto kern = traj3d_grad_kernel<C::NGM, C::NEM, TH>;
+    const size_t sb = (sizeof(Smem3<C::NGM, C::NEM, TH>) + 15) / 16 * 16 +
+                      sizeof(Tan3Work<C::NGM, C::NEM>) * (TH / kG3);
+    int dev = 0, smax = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&smax, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (sb > (size_t)smax) {
+        mm_set_error("the 3D tangent kernel needs %zu bytes of shared memory (limit %d)", sb, smax);
+        return -1;
+    }
+    if (prep_smem(kern, sb)) return -3;
+    const int ngroups = TH / kG3;
+    const long long gx = (T.n_particles + ngroups - 1) / ngroups;
+    kern<<<(unsigned)gx, TH, sb, st>>>(P, T);
+    return mm_cuda_check(cudaGetLastError(), "traj3d_grad_kernel launch") ? -3 : 0;
+}
+
+}  // namespace
+
+extern "C" int mm_traj3d_grad_run(const mm_pack *pack, const mm_beams *beams, const mm_t3grad_opts *opts,
+                                  int64_t n_particles, double *state, double *vsync, int32_t *n_actual,
+                                  int32_t *status, int32_t *n_events, double *ckpt, void *stream)
+{
+    if (!opts) { mm_set_error("3D trajectory-gradient options are required"); return -1; }
+    Force3Params P;
+    if (fill3(pack, beams, opts->hbar, 1, P)) return -1;
+    if (n_particles < 0 || opts->n_steps < 1 || opts->step0 < 0) {
+        mm_set_error("n_particles >= 0, n_steps >= 1, step0 >= 0 required");
+        return -1;
+    }
+    if (n_particles > 0xffffffffLL || opts->step0 + opts->n_steps > 0x7fffffffLL) {
+        mm_set_error("particle and step indices must fit the 32-bit RNG counter words");
+        return -1;
+    }
+    if (opts->n_par < 1 || opts->n_par > MM_TGRAD_MAX_PAR) {
+        mm_set_error("n_par=%d out of range [1, %d]", opts->n_par, MM_TGRAD_MAX_PAR);
+        return -1;
+    }
+    for (int b = 0; b < beams->n_b; b++)
+        if (opts->freq_par[b] < -1 || opts->freq_par[b] >= opts->n_par || opts->s0_par[b] < -1 ||
+            opts->s0_par[b] >= opts->n_par) {
+            mm_set_error("beam %d: parameter index out of range [-1, n_par)", b);
+            return -1;
+        }
+    if (opts->bprime_par < -1 || opts->bprime_par >= opts->n_par) {
+        mm_set_error("bprime_par out of range [-1, n_par)");
+        return -1;
+    }
+    if (ckpt && opts->ckpt_every < 1) { mm_set_error("ckpt needs ckpt_every >= 1"); return -1; }
+    if (n_particles == 0) return 0;
+    if (!state || !vsync || !n_actual || !status) {
+        mm_set_error("state, vsync, n_actual and status must be non-null");
+        return -1;
+    }
+    P.n_points = 0; P.pps = 1; P.r = P.v = nullptr; P.F = P.R = P.pop = nullptr; P.status = nullptr;
+    Tg3Params T;
+    T.dt = opts->dt; T.r_escape = opts->r_escape; T.mass = pack->mass;
+    T.v_rec = P.hbar * P.k / pack->mass;
+    T.gap_tol = opts->gap_tol > 0 ? opts->gap_tol : 1e-9;
+    T.n_particles = n_particles; T.n_steps = opts->n_steps; T.step0 = opts->step0;
+    T.ckpt_every = ckpt ? opts->ckpt_every : 1;
+    T.n_par = opts->n_par; T.kicks = opts->kicks ? 1 : 0; T.bprime_par = opts->bprime_par;
+    T.seed = opts->seed;
+    for (int b = 0; b < NBM; b++) {
+        T.freq_par[b] = (signed char)(b < beams->n_b ? opts->freq_par[b] : -1);
+        T.s0_par[b] = (signed char)(b < beams->n_b ? opts->s0_par[b] : -1);
+    }
+    T.state = state; T.vsync = vsync; T.n_actual = n_actual; T.status = status; T.n_events = n_events;
+    T.ckpt = ckpt;
+    return dispatch3(P.n_g, P.n_e, [&](auto C) -> int {
+        return launch_traj3d_grad<decltype(C)>(P, T, (cudaStream_t)stream);
+    });
+}
+
+extern "C" int64_t mm_traj3d_grad_checkpoints(int64_t step0, int64_t n_steps, int64_t ckpt_every)
+{
+    return t3_checkpoints(step0, n_steps, ckpt_every);
 }

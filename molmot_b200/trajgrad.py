@@ -151,3 +151,70 @@ def mean_kinetic_energy(theta: torch.Tensor, pack: MoleculePack, kdir, freq, pol
     with respect to theta.  run_kw: r_escape, kicks, seed, hbar (traj_grad)."""
     return MeanKineticEnergy.apply(theta, pack, (kdir, freq, pol, s0, bgrad, gamma_eff),
                                    (freq_par, s0_par, bprime_par), r0, v0, dt, n_steps, run_kw)
+
+
+class DegenerateSpectrum(RuntimeError):
+    """A 3D tangent step met a degenerate ground Zeeman spectrum, where the
+    eigenbasis -- and with it d(force)/d(position) -- is not defined."""
+
+
+def traj3d_grad(pack: MoleculePack, beams: BeamSets, r0, v0, dt: float, n_steps: int, *,
+                n_par: int, freq_par=None, s0_par=None, bprime_par: int = -1,
+                r_escape: float = 0.015, kicks: bool = False, seed: int = 0, hbar=None,
+                gap_tol: float = 0.0, step0: int = 0, state=None, n_actual=None,
+                ckpt_every: int = 0, allow_degenerate: bool = False, stream=None) -> dict:
+    """The 3D leapfrog ensemble of ``engine.traj3d`` (24-beam force, beam set
+    0 of 3D beam sets) with its tangents d(r, v)/d theta (mm_traj3d_grad_run),
+    through the field dependence of the ground Zeeman eigenbasis.
+
+    r0, v0: (N, 3) for a new run (tangents start at zero), or ``state``
+    ([N, 6 + 6 n_par]: r, v_half and their tangents, e.g. a checkpoint) with
+    ``step0`` the next update's absolute index and ``n_actual`` the previous
+    call's stop steps.  Returns device tensors r, vh (N, 3), dr, dvh
+    (N, 3, n_par), v and dv (the synchronised velocity of the last update and
+    its tangent), n_actual, status, n_events, state and, with ckpt_every > 0,
+    ckpt.  Raises DegenerateSpectrum when a step met a degenerate spectrum
+    (status bit MM_ST_DEGENERATE), unless allow_degenerate.
+    """
+    from .constants import hbar as HBAR_CODATA
+    if state is None:
+        state = pack_state(r0, v0, n_par=n_par)
+    else:
+        state = _to_dev(state).reshape(-1, 6 + 6 * n_par).clone()
+    N = state.shape[0]
+    dev = state.device
+    if n_actual is None:
+        n_actual = torch.zeros(N, dtype=torch.int32, device=dev)
+    else:
+        n_actual = torch.as_tensor(n_actual, dtype=torch.int32, device=dev).clone()
+    o = _lib.T3gradOpts()
+    o.n_steps, o.step0, o.ckpt_every = int(n_steps), int(step0), int(ckpt_every)
+    o.dt, o.r_escape = float(dt), float(r_escape)
+    o.hbar = float(hbar) if hbar else HBAR_CODATA
+    o.gap_tol = float(gap_tol)
+    o.seed, o.kicks, o.n_par = int(seed), 1 if kicks else 0, int(n_par)
+    o.freq_par = _param_map(freq_par, beams.n_beams, n_par, "freq_par")
+    o.s0_par = _param_map(s0_par, beams.n_beams, n_par, "s0_par")
+    o.bprime_par = int(bprime_par)
+    L = _lib.load()
+    vsync = torch.empty((N, 3 + 3 * n_par), dtype=torch.float64, device=dev)
+    status = torch.empty(N, dtype=torch.int32, device=dev)
+    n_ev = torch.empty(N, dtype=torch.int32, device=dev)
+    ck = None
+    if ckpt_every > 0:
+        n_ck = int(L.mm_traj3d_grad_checkpoints(int(step0), int(n_steps), int(ckpt_every)))
+        ck = torch.empty((n_ck, N, 6 + 6 * n_par), dtype=torch.float64, device=dev)
+    rc = L.mm_traj3d_grad_run(pack.handle, beams.handle, ctypes.byref(o), N, _dptr(state), _dptr(vsync),
+                              _dptr(n_actual), _dptr(status), _dptr(n_ev), _dptr(ck), _stream_handle(stream))
+    _lib.check(rc, "mm_traj3d_grad_run")
+    if not allow_degenerate and bool((status & _lib.MM_ST_DEGENERATE).any()):
+        raise DegenerateSpectrum(
+            "the ground Zeeman spectrum is degenerate on this trajectory (e.g. SrOH's 6 + 6 "
+            "clusters): the eigenbasis, and with it d(force)/d(position), is not defined")
+    out = unpack_state(state, n_par)
+    out["vh"], out["dvh"] = out.pop("v"), out.pop("dv")
+    out.update(v=vsync[:, :3], dv=vsync[:, 3:].reshape(N, 3, n_par), state=state, n_actual=n_actual,
+               status=status, n_events=n_ev)
+    if ck is not None:
+        out["ckpt"] = ck
+    return out

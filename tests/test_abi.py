@@ -87,7 +87,8 @@ def test_option_struct_layouts_match_header(tmp_path):
         pytest.skip("gcc not available")
     pairs = [("mm_mol_desc", _lib.MolDesc), ("mm_beam_desc", _lib.BeamDesc),
              ("mm_batch_opts", _lib.BatchOpts), ("mm_traj_opts", _lib.TrajOpts),
-             ("mm_uneven_opts", _lib.UnevenOpts), ("mm_tgrad_opts", _lib.TgradOpts)]
+             ("mm_uneven_opts", _lib.UnevenOpts), ("mm_tgrad_opts", _lib.TgradOpts),
+             ("mm_t3grad_opts", _lib.T3gradOpts)]
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "molmot_b200.h"', "int main(void) {"]
     for cname, cls in pairs:
         lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
