@@ -17,10 +17,15 @@ e2e        : the same metric through the public API with host arrays: per step
              maps come back device->host into page-locked memory, chunk by
              chunk, overlapped with the computation (inside the timed region).
 roofline   : the force kernel against the measured FP64/FP32 FMA peaks of
-             this GPU (mm_peak_probe); algorithmic FLOPs per point of the form
-             that runs (molmot_b200/flops.py).
-cpu_baseline: the reference's numba core restated (oracle/rate_eq_numba.py)
-             on all host cores, on a bounded sample of the same workload.
+             this GPU (the FMA probe of libmolmot_probe.so); algorithmic FLOPs
+             per point of the form that runs (molmot_b200/flops.py).
+cpu_baseline: the reference's own numba core (_rate_eq_core, from the reference
+             installed in baseline/_ref) on all host cores, on a bounded sample
+             of the same workload, plus a one-thread figure.
+
+Output: three JSON lines -- every measurement (long), then the compact
+evidence line (the other forms, accuracy, trajectories, adjoints, uneven
+batch), then the headline.
 
 `--impl reference` prints the CPU reference arm instead (rank 0 only).
 """
@@ -369,6 +374,12 @@ def secondary_measurements(torch, mol, pack, dev, peaks):
                                     "4-frequency beams, r ~ N(0, 1 mm), v ~ MB(5 mK), Euler dt=1us, "
                                     "recoil kicks at fixed noise, tangents for the 4 detunings, "
                                     "state checkpointed every 50 steps"}
+    # the same gradient through the 24-beam 3D force: SrOH's ground Zeeman
+    # spectrum is degenerate there (the eigenbasis derivative is undefined), so
+    # a non-degenerate synthetic 12 + 4 molecule with the same beam geometry;
+    # 4096 particles x 1000 leapfrog steps, kicks at fixed noise, 4 detunings,
+    # checkpoints every 50 steps
+    out["traj3d_grad"] = traj3d_grad_measurement(torch, dev, sig_v)
     # adjoint: 1024 parameter sets x 66 stencil points (33 z + 33 v)
     kdir, freq, pol, s0, B = make_params(mol, 1024, SEED + 7)
     bsa = BeamSets(kdir, freq, pol, s0, B)
@@ -393,6 +404,38 @@ def secondary_measurements(torch, mol, pack, dev, peaks):
                                   "cost_ratio": tra / trf, "vs_elimination_adjoint": ta / tra}}
     out["uneven"] = uneven_measurement(torch, dev, peaks)
     return out
+
+
+def traj3d_grad_measurement(torch, dev, sig_v):
+    """Particle-steps/s of the 3D trajectory tangents (mm_traj3d_grad_run) and
+    the cost against the forward-only 3D run of the same ensemble."""
+    from molmot_b200.constants import hbar as HBAR_CODATA
+    from molmot_b200.engine import pack_for, traj3d
+    from molmot_b200.molecules.synthetic import synthetic_molecule
+    from molmot_b200.simulator_3d import MOTSimulator3D, make_beam_pairs_dc4
+    from molmot_b200.trajgrad import traj3d_grad
+    m = synthetic_molecule(12, 4, 5)
+    sim = MOTSimulator3D(m, make_beam_pairs_dc4(m, -0.5, 0.5, 1.0), B_gradient=0.2)
+    rng = np.random.default_rng(SEED + 3)
+    N, S = 4096, 1000
+    r0 = torch.as_tensor(rng.normal(0, 1e-3, (N, 3)), device=dev)
+    v0 = torch.as_tensor(rng.normal(0, sig_v, (N, 3)), device=dev)
+    bs, pk = sim._bs(), pack_for(m)
+    fpar = [b // 6 for b in range(24)]
+    run = lambda: traj3d_grad(pk, bs, r0, v0, 1e-6, S, n_par=4, freq_par=fpar, kicks=True, seed=SEED,
+                              ckpt_every=50, allow_degenerate=True)
+    ms = _ev_time(torch, run, 1)
+    msf = _ev_time(torch, lambda: traj3d(pk, bs, r0, v0, 1e-6, S, kicks=True, seed=SEED, hbar=HBAR_CODATA), 1)
+    o = run()
+    alive = (o["r"].norm(dim=1) <= 0.015)
+    g = (m.mass * (o["v"][:, :, None] * o["dv"]).sum(1)[alive].mean(0)).cpu().numpy()
+    return {"metric": "particle-steps/s", "value": N * S / (ms * 1e-3), "particles": N, "steps": S, "ms": ms,
+            "forward_ms": msf, "cost_ratio_vs_forward": ms / msf,
+            "degenerate_particles": int(((o["status"] & 8) != 0).sum()),
+            "dE_ddetuning_J_per_Hz": [float(x) for x in g],
+            "workload": "synthetic 12+4 molecule with a non-degenerate ground Zeeman spectrum, 24-beam "
+                        "3D quadrupole MOT, leapfrog dt=1us, recoil kicks at fixed noise, tangents for "
+                        "the 4 frequency components, checkpoints every 50 steps"}
 
 
 def uneven_measurement(torch, dev, peaks):
@@ -480,6 +523,9 @@ def evidence_line(plain, red64, accuracy, secondary):
         ev["traj1d"] = {"fp64": r(secondary["traj1d"]["value"]), "fp32": r(secondary["traj1d_fp32"]["value"])}
         ev["traj_grad"] = {"value": r(secondary["traj_grad"]["value"]),
                            "vs_forward": r(secondary["traj_grad"]["cost_ratio_vs_fp64_forward"], 3)}
+        t3g = secondary["traj3d_grad"]
+        ev["traj3d_grad"] = {"value": r(t3g["value"]), "ms": r(t3g["ms"]),
+                             "vs_forward": r(t3g["cost_ratio_vs_forward"], 3)}
         ev["adjoint_cost"] = {"fp64": r(secondary["adjoint"]["cost_ratio"], 3),
                               "reduced": r(secondary["adjoint"]["reduced"]["cost_ratio"], 3)}
         ev["uneven"] = {"value": r(u["persistent_value"]), "ms": r(u["persistent_ms"]),
