@@ -468,6 +468,14 @@ def uneven_measurement(torch, dev, peaks):
         singles.append((u, vd[off[i]:off[i + 1]], zd[off[i]:off[i + 1]]))
     ms_s = _ev_time(torch, lambda: [u.force(a, b) for u, a, b in singles], 2)
     pts_s = int(sum(counts[i] for i in sample))
+    # the same sample as one launch per molecule of the plain form (mm_force_batch,
+    # FP64, the reference's elimination), as the reference launches per molecule
+    from molmot_b200.engine import MoleculePack, force_batch
+    plain = [(MoleculePack(mols[i]),
+              BeamSets(kd[i:i + 1], fr[i:i + 1], po[i:i + 1], s0[i:i + 1], Bu[i:i + 1]),
+              vd[off[i]:off[i + 1]], zd[off[i]:off[i + 1]]) for i in sample]
+    ms_pl = _ev_time(torch, lambda: [force_batch(pk, b, a, c, precision="fp64", want_pop=False)
+                                     for pk, b, a, c in plain], 2)
     n = int(off[-1])
     fl = uneven_flops(mols, counts, po)
     achieved = fl / (ms_p * 1e-3) / 1e12
@@ -478,6 +486,7 @@ def uneven_measurement(torch, dev, peaks):
             "persistent_ms": ms_p, "persistent_value": n / (ms_p * 1e-3),
             "graph_replay_ms": ms_g, "warps_per_cta": list(wpc),
             "per_molecule_launches_ms_estimate": ms_s * n / pts_s,
+            "per_molecule_plain_fp64_ms_estimate": ms_pl * n / pts_s,
             "per_molecule_sample": f"{len(sample)} molecules ({pts_s} points), scaled by points",
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": peaks["fp64"],
                          "unit": "TFLOP/s", "frac": achieved / peaks["fp64"],
@@ -530,7 +539,8 @@ def evidence_line(plain, red64, accuracy, secondary):
                               "reduced": r(secondary["adjoint"]["reduced"]["cost_ratio"], 3)}
         ev["uneven"] = {"value": r(u["persistent_value"]), "ms": r(u["persistent_ms"]),
                         "frac_fp64": r(u["roofline"]["frac"], 3), "graph_ms": r(u["graph_replay_ms"]),
-                        "per_molecule_ms": r(u["per_molecule_launches_ms_estimate"])}
+                        "per_molecule_ms": r(u["per_molecule_launches_ms_estimate"]),
+                        "per_molecule_plain_ms": r(u["per_molecule_plain_fp64_ms_estimate"])}
         if "accuracy_vs_oracle" in u:
             ev["uneven"]["acc_vs_oracle"] = r(u["accuracy_vs_oracle"]["max"], 2)
     return ev
@@ -654,6 +664,59 @@ def traj3d_full_run(total_steps, chunk=1000):
     print(json.dumps(line))
 
 
+def profile_case(name):
+    """One small workload of a kernel family, run twice (the second launch is
+    the one to capture), for ncu captures that must stay small:
+      large       -- force maps of a 24 + 6 synthetic molecule (large_force_kernel),
+                     64 sets x 64 x 64 points, plain FP64 and excited-chain forms;
+      traj3d_grad -- 3D tangents, synthetic 12 + 4 molecule, 256 particles x 20 steps;
+      traj_grad   -- per-axis tangents, SrOH, 4096 particles x 50 steps;
+      uneven      -- the 2048-molecule uneven batch, one persistent call."""
+    import torch
+    from molmot_b200.engine import BeamSets, MoleculePack, force_batch, pack_for
+    from molmot_b200.molecules import load_sroh_from_julia
+    from molmot_b200.molecules.synthetic import dc_beams_for, synthetic_molecule
+    dev = torch.device("cuda", 0)
+    rng = np.random.default_rng(SEED)
+    t0 = time.perf_counter()
+    for _ in range(2):
+        if name == "large":
+            m = synthetic_molecule(24, 6, 32)
+            kd, fr, po, s0 = dc_beams_for(m)
+            n = 64
+            bs = BeamSets(np.tile(kd, (n, 1)), fr[None] + rng.uniform(-1e7, 0, (n, 1)), np.tile(po, (n, 1)),
+                          np.tile(s0, (n, 1)), rng.uniform(0.1, 0.4, n))
+            v = torch.as_tensor(np.linspace(-8, 8, 64), device=dev)
+            z = torch.as_tensor(np.linspace(-8e-3, 8e-3, 64), device=dev)
+            for prec in ("fp64", "fp64_reduced"):
+                force_batch(MoleculePack(m), bs, v, z, grid=True, precision=prec, want_pop=False)
+        elif name == "traj3d_grad":
+            from molmot_b200.simulator_3d import MOTSimulator3D, make_beam_pairs_dc4
+            from molmot_b200.trajgrad import traj3d_grad
+            m = synthetic_molecule(12, 4, 5)
+            sim = MOTSimulator3D(m, make_beam_pairs_dc4(m, -0.5, 0.5, 1.0), B_gradient=0.2)
+            r0 = rng.normal(0, 1e-3, (256, 3))
+            v0 = rng.normal(0, 0.6, (256, 3))
+            traj3d_grad(pack_for(m), sim._bs(), r0, v0, 1e-6, 20, n_par=4, freq_par=[b // 6 for b in range(24)],
+                        kicks=True, seed=SEED)
+        elif name == "traj_grad":
+            from molmot_b200.fields import make_dc_mot_beams
+            from molmot_b200.trajgrad import traj_grad
+            mol = load_sroh_from_julia()
+            bs = BeamSets.from_beams(make_dc_mot_beams(mol, -0.20, 0.70, 1.0), 0.16)
+            r0 = rng.normal(0, 1e-3, (4096, 3))
+            v0 = rng.normal(0, 0.6, (4096, 3))
+            traj_grad(pack_for(mol), bs, r0, v0, 1e-6, 50, n_par=4, freq_par=[0, 0, 1, 1, 2, 2, 3, 3],
+                      kicks=True, seed=SEED)
+        elif name == "uneven":
+            from molmot_b200.uneven import MoleculeBank, UnevenBatch, make_uneven_workload
+            mols, counts, (kd, fr, po, s0), Bu, vu, zu = make_uneven_workload(n_mol=2048, seed=SEED)
+            ub = UnevenBatch(MoleculeBank(mols), counts, BeamSets(kd, fr, po, s0, Bu))
+            ub.force(vu, zu)
+        torch.cuda.synchronize()
+    print(json.dumps({"case": name, "seconds": time.perf_counter() - t0}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -664,6 +727,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-secondary", action="store_true",
                     help="skip the trajectory / adjoint measurements (small profiling runs)")
+    ap.add_argument("--case", default="", choices=["", "large", "traj3d_grad", "traj_grad", "uneven"],
+                    help="run one small workload of the named kernel twice and exit (profiling runs)")
     ap.add_argument("--traj3d-full", type=int, default=0, metavar="STEPS",
                     help="instead of the force maps: run the whole 3D ensemble (65,536 particles, "
                          "STEPS leapfrog steps, e.g. 30000) in 1000-step resumed chunks and print "
@@ -673,6 +738,8 @@ def main():
         return run_reference_arm(args)
     if args.traj3d_full:
         return traj3d_full_run(args.traj3d_full)
+    if args.case:
+        return profile_case(args.case)
 
     import torch
     import torch.distributed as dist

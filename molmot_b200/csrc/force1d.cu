@@ -506,12 +506,16 @@ traj1d_reduced_kernel(ForceParams P, TrajParams T)
 // Poisson((R_x + R_y + R_z) dt) events per step, 2N isotropic kicks of
 // hbar k / m (kicks.cuh, counters (particle, absolute step)); under
 // differentiation they are held fixed (the derivative at fixed noise: event
-// counts and directions do not move with theta).  Four lanes per particle:
-// lane a < 3 integrates axis a, lane 3 only joins the sums.  The lanes of a
-// particle share the kick's total rate and the escape radius through
-// shuffles that every lane of the warp executes unconditionally, including
-// lanes without a particle and particles that stopped.  State row per
-// particle (width 6 + 6 n_par): r[3], v[3], Tr[3][n_par], Tv[3][n_par].
+// counts and directions do not move with theta).  Sixteen lanes per
+// particle: four axis slots (x, y, z and an idle one) of kTgSub lanes; the
+// lanes of an axis split the ground states of each force-and-gradient solve
+// and add their partial sums with shuffles (reduced_adjoint_point<..., NL>),
+// then hold the axis' state alike.  The lanes of a particle share the kick's
+// total rate and the escape radius through shuffles; every lane of the warp
+// executes all of these unconditionally, including lanes without a particle,
+// the idle slot and particles that stopped (they solve the point (0, 0)).
+// State row per particle (width 6 + 6 n_par): r[3], v[3], Tr[3][n_par],
+// Tv[3][n_par].
 struct TgParams {
     double dt, r_escape, mass, v_rec;
     long long n_particles, n_steps, step0, ckpt_every;
@@ -525,6 +529,8 @@ struct TgParams {
 
 constexpr int kTgMaxPar = MM_TGRAD_MAX_PAR;
 constexpr int kTgThreads = 128;
+constexpr int kTgSub = 4;             // lanes per axis: each takes every 4th ground state
+constexpr int kTgLanes = 4 * kTgSub;  // lanes per particle: x, y, z and an idle slot
 
 template <int NGMAX, int NEMAX, bool EXACT, int PAD>
 __global__ void __launch_bounds__(kTgThreads, 2)
@@ -538,12 +544,18 @@ traj_grad_kernel(ForceParams P, TgParams T)
     const int nb = P.n_b, st = blockDim.x, np = T.n_par, W = 6 + 6 * np;
     double *fd = (double *)(sm + Ly.total) + threadIdx.x;
     double *gf = fd + (size_t)nb * st, *gs = gf + (size_t)nb * st;
-    const int a = threadIdx.x & 3;
+    const int tl = threadIdx.x % kTgLanes;
+    const int a = tl / kTgSub, jsub = tl % kTgSub;  // axis slot, sub-lane
     const bool axis = a < 3;
-    const long long ip = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 2;
+    const long long ip = ((long long)blockIdx.x * blockDim.x + threadIdx.x) / kTgLanes;
     const bool valid = ip < T.n_particles;
     const double mult = (a < 2) ? -0.5 : 1.0;
     const double Bg = P.bgrad[0] * mult;  // the per-axis model's product (mm_traj_run)
+    // sum over the particle's axis slots (the same sub-lane of each slot)
+    auto axis_sum = [](double v) {
+        v += __shfl_xor_sync(0xffffffffu, v, kTgSub);
+        return v + __shfl_xor_sync(0xffffffffu, v, 2 * kTgSub);
+    };
     double x = 0.0, u = 0.0, Tx[kTgMaxPar], Tv[kTgMaxPar];
     double *row = T.state + (valid ? ip : 0) * W;
 #pragma unroll
@@ -557,7 +569,7 @@ traj_grad_kernel(ForceParams P, TgParams T)
         u = row[3 + a];
     }
     auto write_row = [&](double *dst) {
-        if (valid && axis) {
+        if (valid && axis && jsub == 0) {
             dst[a] = x;
             dst[3 + a] = u;
             for (int k = 0; k < np; k++) {
@@ -568,7 +580,7 @@ traj_grad_kernel(ForceParams P, TgParams T)
     };
     // a particle already beyond r_escape stopped in an earlier call (the sum
     // runs on every lane: it is a warp collective)
-    const double r2_0 = mm_group_sum(x * x, 4);
+    const double r2_0 = axis_sum(x * x);
     const bool stopped = !valid || sqrt(r2_0) > T.r_escape;
     bool done = stopped;
     long long na = -1;
@@ -580,14 +592,17 @@ traj_grad_kernel(ForceParams P, TgParams T)
         double F = 0.0, R = 0.0, dth[kTgMaxPar];
 #pragma unroll
         for (int k = 0; k < kTgMaxPar; k++) dth[k] = 0.0;
-        if (!done && axis) {
-            for (int b = 0; b < nb; b++) {
-                gf[b * st] = 0.0;
-                gs[b * st] = 0.0;
-            }
-            double gBG;
-            const RedOut o = reduced_adjoint_point<NGMAX, NEMAX, EXACT, PAD>(P, S, P.pol, u, x, Bg, fd, st,
-                                                                             gf, gs, gBG);
+        // the solve is shared by the axis' sub-lanes (warp collectives inside):
+        // every lane takes part, stopped particles and the idle slot at (0, 0)
+        const bool act = !done && axis;
+        for (int b = 0; b < nb; b++) {
+            gf[b * st] = 0.0;
+            gs[b * st] = 0.0;
+        }
+        double gBG;
+        const RedOut o = reduced_adjoint_point<NGMAX, NEMAX, EXACT, PAD, kTgSub>(
+            P, S, P.pol, act ? u : 0.0, act ? x : 0.0, Bg, fd, st, gf, gs, gBG, jsub);
+        if (act) {
             F = o.F;
             R = o.R;
             double dv = 0.0;
@@ -610,11 +625,10 @@ traj_grad_kernel(ForceParams P, TgParams T)
         // warp collectives below: every lane, every iteration
         double kick[3] = {0.0, 0.0, 0.0};
         if (T.kicks) {  // uniform over the grid
-            const double Rt = (R + __shfl_xor_sync(0xffffffffu, R, 1)) +
-                              (__shfl_xor_sync(0xffffffffu, R, 2) + __shfl_xor_sync(0xffffffffu, R, 3));
+            const double Rt = axis_sum(act ? R : 0.0);
             if (!done) recoil_kick(T.seed, (unsigned)ip, (unsigned)j, Rt * T.dt, T.v_rec, kick);
         }
-        if (!done && axis) {
+        if (act) {
             const double acc = __ddiv_rn(F, T.mass);
             u = __dadd_rn(u, __dmul_rn(acc, T.dt));
             if (T.kicks) u = __dadd_rn(u, kick[a]);
@@ -626,7 +640,7 @@ traj_grad_kernel(ForceParams P, TgParams T)
                 Tx[k] = fma(Tv[k], T.dt, Tx[k]);
             }
         }
-        const double r2 = mm_group_sum(x * x, 4);
+        const double r2 = axis_sum(x * x);
         if (!done && sqrt(r2) > T.r_escape) {
             na = j;
             done = true;
@@ -644,7 +658,7 @@ traj_grad_kernel(ForceParams P, TgParams T)
                 n_ck++;
             }
     write_row(row);
-    if (valid && a == 0) {
+    if (valid && tl == 0) {
         if (na >= 0) T.n_actual[ip] = (int32_t)na;
         else if (!stopped) T.n_actual[ip] = (int32_t)jend;
     }
@@ -797,7 +811,7 @@ int launch_traj_grad(const ForceParams &P, const TgParams &T, cudaStream_t st)
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb);
         if (mm_cuda_check(e, "cudaFuncSetAttribute")) return -3;
     }
-    const long long gx = (4 * T.n_particles + kTgThreads - 1) / kTgThreads;
+    const long long gx = ((long long)kTgLanes * T.n_particles + kTgThreads - 1) / kTgThreads;
     kern<<<(unsigned)gx, kTgThreads, sb, st>>>(P, T);
     return mm_cuda_check(cudaGetLastError(), "traj_grad_kernel launch") ? -3 : 0;
 }

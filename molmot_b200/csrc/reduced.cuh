@@ -610,11 +610,24 @@ __device__ __forceinline__ void reduced_point2(const ForceParams &P, const RedVi
 // gf[b * stride], gs[b * stride]: this thread's per-beam accumulators
 // (shared memory); the caller zeroes them.  pol: the set's polarisations.
 // Valid sets only (S.valid); finite v and z.
-template <int NGMAX, int NEMAX, bool EXACT, int PAD>
+// NL > 1: the point is shared by NL consecutive lanes (sub-lane j), each
+// taking the ground states g = j (mod NL) in both passes; the partial sums
+// (K, cw, cf after the first pass, the per-beam accumulators and dF/dB after
+// the second) are added over the NL lanes with shuffles, so every lane ends
+// with the whole result.  All lanes of the warp must call it together.
+template <int NL>
+__device__ __forceinline__ double red_lane_sum(double x)
+{
+#pragma unroll
+    for (int o = 1; o < NL; o <<= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    return x;
+}
+
+template <int NGMAX, int NEMAX, bool EXACT, int PAD, int NL = 1>
 __device__ __forceinline__ RedOut reduced_adjoint_point(const ForceParams &P, const RedView &S,
                                                         const int32_t *pol, double v, double z,
                                                         double Bgrad, double *fd, int stride,
-                                                        double *gf, double *gs, double &gBG)
+                                                        double *gf, double *gs, double &gBG, int j = 0)
 {
     const int n_g = EXACT ? NGMAX : P.n_g;
     const int n_e = EXACT ? NEMAX : P.n_e;
@@ -640,7 +653,7 @@ __device__ __forceinline__ RedOut reduced_adjoint_point(const ForceParams &P, co
 #pragma unroll
         for (int e2 = 0; e2 < NEMAX; e2++) K[e][e2] = 0.0;
     }
-    for (int g = 0; g < n_g; g++) {
+    for (int g = j; g < n_g; g += NL) {
         double Re[NEMAX], f, s;
         reduced_rates<NEMAX, PAD, true>(S, g, C, gh2, Re, f, s);
         double rt = 0.0;
@@ -657,10 +670,19 @@ __device__ __forceinline__ RedOut reduced_adjoint_point(const ForceParams &P, co
             for (int e2 = 0; e2 < NEMAX; e2++) K[e2][e] = fma(Re[e2] * inv, br, K[e2][e]);
         }
     }
+    if constexpr (NL > 1) {
+#pragma unroll
+        for (int e = 0; e < NEMAX; e++) {
+            cw[e] = red_lane_sum<NL>(cw[e]);
+            cf[e] = red_lane_sum<NL>(cf[e]);
+#pragma unroll
+            for (int e2 = 0; e2 < NEMAX; e2++) K[e][e2] = red_lane_sum<NL>(K[e][e2]);
+        }
+    }
 #pragma unroll
     for (int i = 0; i < NEMAX; i++)
 #pragma unroll
-        for (int j = 0; j < NEMAX; j++) K0[i][j] = K[i][j];
+        for (int jj = 0; jj < NEMAX; jj++) K0[i][jj] = K[i][jj];
     double pi[NEMAX];
     const bool ok = gth_stationary<NEMAX>(K, n_e, pi);
     double nrm = 0.0, fn = 0.0, rn = 0.0;
@@ -713,7 +735,7 @@ __device__ __forceinline__ RedOut reduced_adjoint_point(const ForceParams &P, co
     // second pass: per ground state coefficients, then the triples once more
     gBG = 0.0;
     const double inrm = in, Fin = F * in;
-    for (int g = 0; g < n_g; g++) {
+    for (int g = j; g < n_g; g += NL) {
         double Re[NEMAX], f, s;
         reduced_rates<NEMAX, PAD, true>(S, g, C, gh2, Re, f, s);
         double rt = 0.0, yg = 0.0;
@@ -753,6 +775,13 @@ __device__ __forceinline__ RedOut reduced_adjoint_point(const ForceParams &P, co
                 gs[b * stride] = fma(qs, L, gs[b * stride]);
                 gBG = fma(q * dLd, dBde, gBG);
             }
+        }
+    }
+    if constexpr (NL > 1) {
+        gBG = red_lane_sum<NL>(gBG);
+        for (int b = 0; b < P.n_b; b++) {
+            gf[b * stride] = red_lane_sum<NL>(gf[b * stride]);
+            gs[b * stride] = red_lane_sum<NL>(gs[b * stride]);
         }
     }
     RedOut o;
