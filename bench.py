@@ -49,7 +49,7 @@ METRIC = "16-level steady-state force evals/s and particle-steps/s: plain FP64 v
 N_SETS, NV, NZ = 4096, 256, 256
 # dram__bytes_read.sum + dram__bytes_write.sum per point of force_reduced_kernel
 # (FP32 form, grid layout, F only), from an ncu capture of a 512-set launch
-TRAFFIC_PER_POINT = 2.2315e9 / (4096 * 256 * 256)
+TRAFFIC_PER_POINT = (416000 + 266039552) / (512 * 256 * 256)
 SEED = 20261203
 
 
@@ -669,6 +669,7 @@ def profile_case(name):
     the one to capture), for ncu captures that must stay small:
       large       -- force maps of a 24 + 6 synthetic molecule (large_force_kernel),
                      64 sets x 64 x 64 points, plain FP64 and excited-chain forms;
+      traj3d      -- the SrOH 3D ensemble (traj3d_kernel), 8192 particles x 24 steps;
       traj3d_grad -- 3D tangents, synthetic 12 + 4 molecule, 256 particles x 20 steps;
       traj_grad   -- per-axis tangents, SrOH, 4096 particles x 50 steps;
       uneven      -- the 2048-molecule uneven batch, one persistent call."""
@@ -699,6 +700,15 @@ def profile_case(name):
             v0 = rng.normal(0, 0.6, (256, 3))
             traj3d_grad(pack_for(m), sim._bs(), r0, v0, 1e-6, 20, n_par=4, freq_par=[b // 6 for b in range(24)],
                         kicks=True, seed=SEED)
+        elif name == "traj3d":
+            from molmot_b200.constants import hbar as HBAR_CODATA
+            from molmot_b200.engine import traj3d
+            from molmot_b200.simulator_3d import MOTSimulator3D, make_beam_pairs_dc4
+            mol = load_sroh_from_julia()
+            sim = MOTSimulator3D(mol, make_beam_pairs_dc4(mol, -0.30, 0.40, 1.0), B_gradient=0.16)
+            r0 = rng.normal(0, 1e-3, (8192, 3))
+            v0 = rng.normal(0, 0.6, (8192, 3))
+            traj3d(pack_for(mol), sim._bs(), r0, v0, 1e-6, 24, kicks=True, seed=SEED, hbar=HBAR_CODATA)
         elif name == "traj_grad":
             from molmot_b200.fields import make_dc_mot_beams
             from molmot_b200.trajgrad import traj_grad
@@ -727,7 +737,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-secondary", action="store_true",
                     help="skip the trajectory / adjoint measurements (small profiling runs)")
-    ap.add_argument("--case", default="", choices=["", "large", "traj3d_grad", "traj_grad", "uneven"],
+    ap.add_argument("--case", default="", choices=["", "large", "traj3d", "traj3d_grad", "traj_grad", "uneven"],
                     help="run one small workload of the named kernel twice and exit (profiling runs)")
     ap.add_argument("--traj3d-full", type=int, default=0, metavar="STEPS",
                     help="instead of the force maps: run the whole 3D ensemble (65,536 particles, "

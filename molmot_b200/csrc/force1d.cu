@@ -506,11 +506,13 @@ traj1d_reduced_kernel(ForceParams P, TrajParams T)
 // Poisson((R_x + R_y + R_z) dt) events per step, 2N isotropic kicks of
 // hbar k / m (kicks.cuh, counters (particle, absolute step)); under
 // differentiation they are held fixed (the derivative at fixed noise: event
-// counts and directions do not move with theta).  Sixteen lanes per
-// particle: four axis slots (x, y, z and an idle one) of kTgSub lanes; the
-// lanes of an axis split the ground states of each force-and-gradient solve
-// and add their partial sums with shuffles (reduced_adjoint_point<..., NL>),
-// then hold the axis' state alike.  The lanes of a particle share the kick's
+// counts and directions do not move with theta).  Per particle four axis
+// slots (x, y, z and an idle one) of kTgSub lanes; with kTgSub > 1 the lanes
+// of an axis split the ground states of each force-and-gradient solve and
+// add their partial sums with shuffles (reduced_adjoint_point<..., NL>),
+// then hold the axis' state alike.  One lane per axis was the fastest on
+// 4096 SrOH particles x 1000 steps (33.5 ms; two lanes 38.2 ms, four 49.5 ms:
+// the split adds shuffles and leaves fewer particles per warp).  The lanes of a particle share the kick's
 // total rate and the escape radius through shuffles; every lane of the warp
 // executes all of these unconditionally, including lanes without a particle,
 // the idle slot and particles that stopped (they solve the point (0, 0)).
@@ -529,7 +531,7 @@ struct TgParams {
 
 constexpr int kTgMaxPar = MM_TGRAD_MAX_PAR;
 constexpr int kTgThreads = 128;
-constexpr int kTgSub = 4;             // lanes per axis: each takes every 4th ground state
+constexpr int kTgSub = 1;             // lanes per axis (each takes every kTgSub-th ground state)
 constexpr int kTgLanes = 4 * kTgSub;  // lanes per particle: x, y, z and an idle slot
 
 template <int NGMAX, int NEMAX, bool EXACT, int PAD>

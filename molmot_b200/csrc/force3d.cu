@@ -10,11 +10,11 @@
 //
 // One point per group of 16 lanes (two per warp).  Per point:
 //  1. B = B'(-x/2, -y/2, z) 1e4 G;  H = B.Z (ground block), Hermitianised.
-//  2. Cyclic Jacobi eigen-decomposition of the complex Hermitian H in shared
-//     memory, round-robin (circle) ordering: the n/2 disjoint rotations of a
-//     round are computed by n/2 lanes and applied by all 16 lanes.  Sweeps
-//     continue until the off-diagonal norm is below 1e-30 of the diagonal
-//     norm (warp-uniform).  Eigenvalues are sorted ascending with their
+//  2. Eigen-decomposition of the complex Hermitian H in shared memory
+//     (hermitian_eigen): Householder reduction to tridiagonal form (a lane per
+//     row), a phase change to a real tridiagonal matrix and implicit QL
+//     iterations that every lane runs on its own copy, rotating its own row
+//     of the eigenvector matrix.  Eigenvalues are sorted ascending with their
 //     vectors, as numpy.linalg.eigh returns them; Es_g[i] = E_g[i] + lambda_i.
 //  3. |U^H |tdm||^2 per (eigenstate, e, q); branching ratios.
 //  4. Lane g accumulates, over beams and excited states, the unsaturated rates,
@@ -82,11 +82,9 @@ struct Smem3 {
     double E[NGM + NEM], Ze[NEM];
     double khat[NBM][3], freq[NBM], s0[NBM], radius[NBM];
     int pol[NBM];
-    unsigned short sched[NGM - 1][NGM / 2];  // circle schedule: p | q << 8 of round r, slot i
     struct GroupBody {
         double Hre[NGM * LDH], Him[NGM * LDH];
         double Vre[NGM * LDH], Vim[NGM * LDH];
-        double rot[NGM / 2][3];      // c, Re s, Im s
         double lam[NGM];
         int perm[NGM];
         double dsq[NEM * 3 * NGM];   // |U^H d|^2 at [(e * 3 + q) * NGM + a]: lanes a read consecutive doubles
@@ -110,14 +108,6 @@ __device__ __forceinline__ double gsum16(double x)
 }
 
 
-// Player at position j in round r of the circle schedule on NGM players:
-// position 0 stays, the others rotate; slot i pairs positions i and NGM-1-i.
-template <int NGM>
-__host__ __device__ constexpr int rr_player(int r, int j)
-{
-    return j == 0 ? 0 : ((r + j - 1) % (NGM - 1)) + 1;
-}
-
 template <int NGM, int NEM, int TH>
 __device__ void load_consts3(const Force3Params &P, int set, Smem3<NGM, NEM, TH> &S)
 {
@@ -128,10 +118,6 @@ __device__ void load_consts3(const Force3Params &P, int set, Smem3<NGM, NEM, TH>
         S.Zim[a][rc] = P.Zim[i];
     }
     for (int i = tid; i < n_g * n_e * 3; i += nt) S.tdm[i] = P.tdm[i];
-    for (int i = tid; i < (NGM - 1) * (NGM / 2); i += nt) {
-        const int r = i / (NGM / 2), k = i % (NGM / 2);
-        S.sched[r][k] = (unsigned short)(rr_player<NGM>(r, k) | rr_player<NGM>(r, NGM - 1 - k) << 8);
-    }
     for (int i = tid; i < n_g + n_e; i += nt) S.E[i] = P.E[i];
     for (int i = tid; i < n_e; i += nt) S.Ze[i] = P.Ze[i];
     const size_t o = (size_t)set * n_b;
@@ -161,81 +147,198 @@ struct Keep3 {
 };
 
 
-// One round of NGM/2 disjoint complex Jacobi rotations (H <- J^H H J,
-// V <- V J, J = [[c, s], [-conj(s), c]] on columns p, q).  pq[i] holds the
-// players of slot i of this round (p | q << 8).  Lanes 0..NGM/2-1 compute the
-// rotations; then lane t updates row t of H and V (columns p, q of every
-// pair) and column t of H (rows p, q).  The round index is a run-time value
-// (one copy of this code serves the NGM - 1 rounds); the pair loop is
-// unrolled.
+// Eigen-decomposition of the Hermitian H held in W.Hre / W.Him (rows and
+// columns < n; lane t owns row t), by the standard route of Householder
+// reduction to a Hermitian tridiagonal matrix, a diagonal phase change to a
+// real symmetric tridiagonal one, and implicit QL iterations with Wilkinson
+// shifts (Golub & Van Loan, Matrix Computations, 4th ed., sections 8.3.1
+// and 8.3.5).  On entry W.Vre / W.Vim hold the identity; on exit column j of
+// V is the unit eigenvector of eigenvalue lam_j (V = Q D Z: Q the product of
+// the reflections, D the phases, Z the QL rotations), and the eigenvalues are
+// sorted ascending (ties by index) into W.lam with W.perm[rank] = column, as
+// numpy.linalg.eigh returns the spectrum.  Returns false when an eigenvalue
+// needed more than 60 QL iterations.
+//  * Reduction: lane i < n holds row i.  For column k the reflection
+//    P = I - 2 v v^H (|v| = 1) maps H[k+1 .., k] to (alpha, 0, ..),
+//    alpha = -e^{i arg H[k+1][k]} |H[k+1 .., k]|; the trailing block becomes
+//    H - 2 v w^H - 2 w v^H with w = p - (v^H p) v, p = H v, and Q <- Q P.
+//  * QL: every lane runs the same scalar recurrences on its own copy of the
+//    diagonal d and off-diagonal e and applies each rotation to its own row
+//    of Z, so the lanes need no communication in this phase.
 template <int NGM, class GroupT>
-__device__ __forceinline__ void jacobi_round(GroupT &W, int t, const unsigned short *pq)
+__device__ bool hermitian_eigen(GroupT &W, int t, int n)
 {
-    constexpr int NP = NGM / 2, LDH = NGM + 1;
-    if (t < NP) {
-        const int p = pq[t] & 0xff, q = pq[t] >> 8;
-        double c = 1.0, sr = 0.0, si = 0.0;
-        const double a = W.Hre[p * LDH + p], b = W.Hre[q * LDH + q];
-        const double xr = W.Hre[p * LDH + q], xi = W.Him[p * LDH + q];
-        const double r2 = xr * xr + xi * xi;  // |H_pq|^2
-        const double ab = fabs(a) + fabs(b);
-        if (r2 > 1e-300 && r2 > 1e-36 * ab * ab) {
-            // tau = (b - a) / (2 |H_pq|), t = sign(tau) / (|tau| + sqrt(1 + tau^2)),
-            // c = 1 / sqrt(1 + t^2), s = t c e^{i arg H_pq}
-            const double irho = mm_rsqrt(r2);
-            const double tau = 0.5 * (b - a) * irho;
-            const double q1 = fma(tau, tau, 1.0);
-            const double tt = copysign(mm_rcp(fabs(tau) + q1 * mm_rsqrt(q1)), tau);
-            c = mm_rsqrt(fma(tt, tt, 1.0));
-            const double sv = tt * c * irho;
-            sr = sv * xr;
-            si = sv * xi;
+    constexpr int LDH = NGM + 1;
+    const bool row = t < n;
+    // the Householder vector v and w = H v - (v^H H v) v live in W.dsq, which
+    // is filled only after the decomposition (4 NGM <= NEM 3 NGM doubles)
+    static_assert(sizeof(W.dsq) >= 4 * NGM * sizeof(double), "scratch for v and w");
+    double *hvr = W.dsq, *hvi = hvr + NGM, *hwr = hvi + NGM, *hwi = hwr + NGM;
+    // every step runs on every lane of the warp: the two 16-lane groups of a
+    // warp hold different points and reach the shuffles and __syncwarp()
+    // below together whatever their matrices; a column that is already
+    // tridiagonal gets v = 0, a no-op reflection
+    for (int k = 0; k + 2 < n; k++) {
+        double xr = 0.0, xi = 0.0;
+        if (t > k && row) { xr = W.Hre[t * LDH + k]; xi = W.Him[t * LDH + k]; }
+        const double rest = gsum16((t > k + 1) ? xr * xr + xi * xi : 0.0);
+        const bool act = rest > 0.0;  // the same on the 16 lanes of a group
+        const double x0r = W.Hre[(k + 1) * LDH + k], x0i = W.Him[(k + 1) * LDH + k];
+        const double a0 = sqrt(x0r * x0r + x0i * x0i);
+        const double nx = sqrt(fma(a0, a0, rest));
+        const double phr = (a0 > 0.0) ? x0r / a0 : 1.0, phi = (a0 > 0.0) ? x0i / a0 : 0.0;
+        // v = x - alpha e1 = x + ph nx e1, normalised: |v|^2 = rest + (a0 + nx)^2
+        const double iv = act ? 1.0 / sqrt(fma(a0 + nx, a0 + nx, rest)) : 0.0;
+        if (t > k && row) {
+            double vr = xr, vi = xi;
+            if (t == k + 1) { vr = phr * (a0 + nx); vi = phi * (a0 + nx); }
+            hvr[t] = vr * iv;
+            hvi[t] = vi * iv;
         }
-        W.rot[t][0] = c; W.rot[t][1] = sr; W.rot[t][2] = si;
+        __syncwarp();
+        // p = H v over the trailing block (lane i: row i), K = v^H p
+        double pr = 0.0, pi = 0.0;
+        if (t > k && row) {
+            for (int j = k + 1; j < n; j++) {
+                const double hr = W.Hre[t * LDH + j], hi = W.Him[t * LDH + j];
+                pr += hr * hvr[j] - hi * hvi[j];
+                pi += hr * hvi[j] + hi * hvr[j];
+            }
+        }
+        const double vtr = (t > k && row) ? hvr[t] : 0.0, vti = (t > k && row) ? hvi[t] : 0.0;
+        const double Kv = gsum16(vtr * pr + vti * pi);  // Re(conj(v) p); the imaginary part is zero
+        const double wr = pr - Kv * vtr, wi = pi - Kv * vti;
+        if (t > k && row) { hwr[t] = wr; hwi[t] = wi; }
+        __syncwarp();
+        // trailing block: H[i][j] -= 2 (v_i conj(w_j) + w_i conj(v_j)); column k: (alpha, 0, ..)
+        if (t > k && row) {
+            for (int j = k + 1; j < n; j++) {
+                const double ar = vtr * hwr[j] + vti * hwi[j], ai = vti * hwr[j] - vtr * hwi[j];
+                const double br = wr * hvr[j] + wi * hvi[j], bi = wi * hvr[j] - wr * hvi[j];
+                W.Hre[t * LDH + j] -= 2.0 * (ar + br);
+                W.Him[t * LDH + j] -= 2.0 * (ai + bi);
+            }
+            if (act) {
+                const double alr = -phr * nx, ali = -phi * nx;
+                const double cr = (t == k + 1) ? alr : 0.0, ci = (t == k + 1) ? ali : 0.0;
+                W.Hre[t * LDH + k] = cr; W.Him[t * LDH + k] = ci;
+                W.Hre[k * LDH + t] = cr; W.Him[k * LDH + t] = -ci;
+            }
+        }
+        // Q <- Q P on every row r < n: Q[r][j] -= 2 (Q v)_r conj(v_j)
+        if (row) {
+            double qr = 0.0, qi = 0.0;
+            for (int j = k + 1; j < n; j++) {
+                const double ur = W.Vre[t * LDH + j], ui = W.Vim[t * LDH + j];
+                qr += ur * hvr[j] - ui * hvi[j];
+                qi += ur * hvi[j] + ui * hvr[j];
+            }
+            for (int j = k + 1; j < n; j++) {
+                W.Vre[t * LDH + j] -= 2.0 * (qr * hvr[j] + qi * hvi[j]);
+                W.Vim[t * LDH + j] -= 2.0 * (qi * hvr[j] - qr * hvi[j]);
+            }
+        }
+        __syncwarp();
     }
-    __syncwarp();
-    if (t < NGM) {
-        // columns p, q of H and V in row t:  a_p' = a_p c - a_q conj(s);  a_q' = a_p s + a_q c
+    // real symmetric tridiagonal: d_i = H[i][i], e_i = |H[i+1][i]|, phases
+    // delta_0 = 1, delta_{i+1} = delta_i H[i+1][i] / |H[i+1][i]|
+    double d[NGM], e[NGM], dr[NGM], di[NGM], z[NGM];
+    double cr = 1.0, ci = 0.0;
 #pragma unroll
-        for (int i = 0; i < NP; i++) {
-            const int p = pq[i] & 0xff, q = pq[i] >> 8;
-            const double c = W.rot[i][0], sr = W.rot[i][1], si = W.rot[i][2];
-#pragma unroll
-            for (int m = 0; m < 2; m++) {
-                double *Xr = (m ? W.Vre : W.Hre) + t * LDH, *Xi = (m ? W.Vim : W.Him) + t * LDH;
-                const double apr = Xr[p], api = Xi[p], aqr = Xr[q], aqi = Xi[q];
-                Xr[p] = apr * c - (aqr * sr + aqi * si);
-                Xi[p] = api * c - (aqi * sr - aqr * si);
-                Xr[q] = (apr * sr - api * si) + aqr * c;
-                Xi[q] = (apr * si + api * sr) + aqi * c;
+    for (int i = 0; i < NGM; i++) {
+        d[i] = (i < n) ? W.Hre[i * LDH + i] : 0.0;
+        dr[i] = cr;
+        di[i] = ci;
+        e[i] = 0.0;
+        z[i] = (i == t) ? 1.0 : 0.0;
+        if (i + 1 < n) {
+            const double hr = W.Hre[(i + 1) * LDH + i], hi = W.Him[(i + 1) * LDH + i];
+            const double a = sqrt(hr * hr + hi * hi);
+            e[i] = a;
+            if (a > 0.0) {
+                const double ur = hr / a, ui = hi / a;
+                const double nr = cr * ur - ci * ui;
+                ci = cr * ui + ci * ur;
+                cr = nr;
             }
         }
     }
+    // implicit QL with Wilkinson shifts; lane t applies the rotations to row t of Z
+    bool ok = true;
+    for (int l = 0; l < n; l++) {
+        for (int iter = 0;; iter++) {
+            int m = l;
+            for (; m + 1 < n; m++) {
+                const double dd = fabs(d[m]) + fabs(d[m + 1]);
+                if (fabs(e[m]) <= 2.220446049250313e-16 * dd) break;
+            }
+            if (m == l) break;
+            if (iter == 60) { ok = false; break; }
+            double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
+            double r = sqrt(fma(g, g, 1.0));
+            g = d[m] - d[l] + e[l] / (g + copysign(r, g));
+            double s = 1.0, c = 1.0, p = 0.0;
+            int i = m - 1;
+            for (; i >= l; i--) {
+                const double f = s * e[i], b = c * e[i];
+                r = sqrt(fma(f, f, g * g));
+                e[i + 1] = r;
+                if (r == 0.0) {  // deflation: the rotation vanished
+                    d[i + 1] -= p;
+                    e[m] = 0.0;
+                    break;
+                }
+                s = f / r;
+                c = g / r;
+                g = d[i + 1] - p;
+                r = (d[i] - g) * s + 2.0 * c * b;
+                p = s * r;
+                d[i + 1] = g + p;
+                g = c * r - b;
+                const double z1 = z[i + 1];
+                z[i + 1] = fma(s, z[i], c * z1);
+                z[i] = fma(c, z[i], -s * z1);
+            }
+            if (r == 0.0 && i >= l) continue;
+            d[l] -= p;
+            e[l] = g;
+            e[m] = 0.0;
+        }
+    }
     __syncwarp();
-    if (t < NGM) {
-        // rows p, q of H in column t:  a_p' = c a_p - s a_q;  a_q' = conj(s) a_p + c a_q
+    // Z rows to shared memory (over H, no longer needed), then V <- Q D Z
+    if (row)
+        for (int j = 0; j < n; j++) W.Hre[t * LDH + j] = z[j];
+    __syncwarp();
+    if (row) {
+        double qr[NGM], qi[NGM];
 #pragma unroll
-        for (int i = 0; i < NP; i++) {
-            const int p = pq[i] & 0xff, q = pq[i] >> 8;
-            const double c = W.rot[i][0], sr = W.rot[i][1], si = W.rot[i][2];
-            const double apr = W.Hre[p * LDH + t], api = W.Him[p * LDH + t];
-            const double aqr = W.Hre[q * LDH + t], aqi = W.Him[q * LDH + t];
-            W.Hre[p * LDH + t] = c * apr - (sr * aqr - si * aqi);
-            W.Him[p * LDH + t] = c * api - (sr * aqi + si * aqr);
-            W.Hre[q * LDH + t] = (sr * apr + si * api) + c * aqr;
-            W.Him[q * LDH + t] = (sr * api - si * apr) + c * aqi;
+        for (int k = 0; k < NGM; k++) {  // Q[t][k] delta_k
+            const double ur = (k < n) ? W.Vre[t * LDH + k] : 0.0, ui = (k < n) ? W.Vim[t * LDH + k] : 0.0;
+            qr[k] = ur * dr[k] - ui * di[k];
+            qi[k] = ur * di[k] + ui * dr[k];
         }
+        for (int j = 0; j < n; j++) {
+            double ar = 0.0, ai = 0.0;
+#pragma unroll
+            for (int k = 0; k < NGM; k++)
+                if (k < n) {
+                    const double zk = W.Hre[k * LDH + j];
+                    ar = fma(qr[k], zk, ar);
+                    ai = fma(qi[k], zk, ai);
+                }
+            W.Vre[t * LDH + j] = ar;
+            W.Vim[t * LDH + j] = ai;
+        }
+        // ascending order (ties by index)
+        int rank = 0;
+        const double lt = d[t];
+        for (int j = 0; j < n; j++) rank += (d[j] < lt || (d[j] == lt && j < t)) ? 1 : 0;
+        W.perm[rank] = t;
+        W.lam[rank] = lt;
     }
     __syncwarp();
-    if (t < NP) {  // exact zero of the rotated pair, real diagonal
-        const int p = pq[t] & 0xff, q = pq[t] >> 8;
-        if (W.rot[t][1] != 0.0 || W.rot[t][2] != 0.0) {
-            W.Hre[p * LDH + q] = 0.0; W.Him[p * LDH + q] = 0.0;
-            W.Hre[q * LDH + p] = 0.0; W.Him[q * LDH + p] = 0.0;
-            W.Him[p * LDH + p] = 0.0; W.Him[q * LDH + q] = 0.0;
-        }
-    }
-    __syncwarp();
+    return ok;
 }
 
 // The 3D force at (r, v) for the group of 16 lanes (lane t, base gbase).
@@ -283,36 +386,8 @@ __device__ Out3 force3d_point(const Force3Params &P, Smem3<NGM, NEM, TH> &S,
     }
     __syncwarp();
 
-    // 2. cyclic Jacobi, circle ordering with a compile-time schedule
-    for (int sweep = 0; sweep < 30; sweep++) {
-        // convergence: off-diagonal vs diagonal squared norms (lane t: row t)
-        double off = 0.0, dia = 0.0;
-        if (t < NGM) {
-#pragma unroll
-            for (int j = 0; j < NGM; j++) {
-                const double a2 = W.Hre[t * LDH + j] * W.Hre[t * LDH + j] + W.Him[t * LDH + j] * W.Him[t * LDH + j];
-                if (j == t) dia += a2; else off += a2;
-            }
-        }
-        off = gsum16(off);
-        dia = gsum16(dia);
-        const bool more = off > 1e-30 * dia && off > 1e-300;
-        if (!__any_sync(FULL, more)) break;
-#pragma unroll 1
-        for (int rnd = 0; rnd < NGM - 1; rnd++) jacobi_round<NGM>(W, t, S.sched[rnd]);
-    }
-    // ascending order (ties by index), as eigh returns the spectrum
-    if (t < n_g) {
-        const double lt = W.Hre[t * LDH + t];
-        int rank = 0;
-        for (int j = 0; j < n_g; j++) {
-            const double lj = W.Hre[j * LDH + j];
-            rank += (lj < lt || (lj == lt && j < t)) ? 1 : 0;
-        }
-        W.perm[rank] = t;
-        W.lam[rank] = lt;
-    }
-    __syncwarp();
+    // 2. eigenvalues (ascending) and eigenvectors of the ground Zeeman block
+    if (!hermitian_eigen<NGM>(W, t, n_g)) stat |= MM_ST_NONFINITE;
     // 3. energies and |U^H d|^2 in the eigenbasis (lane a = sorted eigenstate)
     if (t < n_g) W.Esg[t] = S.E[t] + W.lam[t] * G / (2 * MM_PI);
     if (t < n_e)  // exact order of simulator_3d.py:241-243
