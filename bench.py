@@ -672,7 +672,8 @@ def profile_case(name):
       traj3d      -- the SrOH 3D ensemble (traj3d_kernel), 8192 particles x 24 steps;
       traj3d_grad -- 3D tangents, synthetic 12 + 4 molecule, 256 particles x 20 steps;
       traj_grad   -- per-axis tangents, SrOH, 4096 particles x 50 steps;
-      uneven      -- the 2048-molecule uneven batch, one persistent call."""
+      uneven      -- the 2048-molecule uneven batch, one persistent call;
+      adjoint     -- the FP64 elimination adjoint, 1024 SrOH sets x 66 stencil points."""
     import torch
     from molmot_b200.engine import BeamSets, MoleculePack, force_batch, pack_for
     from molmot_b200.molecules import load_sroh_from_julia
@@ -718,6 +719,13 @@ def profile_case(name):
             v0 = rng.normal(0, 0.6, (4096, 3))
             traj_grad(pack_for(mol), bs, r0, v0, 1e-6, 50, n_par=4, freq_par=[0, 0, 1, 1, 2, 2, 3, 3],
                       kicks=True, seed=SEED)
+        elif name == "adjoint":
+            from molmot_b200.engine import force_adjoint
+            mol = load_sroh_from_julia()
+            bsa = BeamSets(*make_params(mol, 1024, SEED + 7))
+            v = np.tile(np.concatenate([np.zeros(33), np.linspace(-0.1, 0.1, 33)]), 1024)
+            z = np.tile(np.concatenate([np.linspace(-0.3e-3, 0.3e-3, 33), np.zeros(33)]), 1024)
+            force_adjoint(pack_for(mol), bsa, v, z, points_per_set=66)
         elif name == "uneven":
             from molmot_b200.uneven import MoleculeBank, UnevenBatch, make_uneven_workload
             mols, counts, (kd, fr, po, s0), Bu, vu, zu = make_uneven_workload(n_mol=2048, seed=SEED)
@@ -737,7 +745,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-secondary", action="store_true",
                     help="skip the trajectory / adjoint measurements (small profiling runs)")
-    ap.add_argument("--case", default="", choices=["", "large", "traj3d", "traj3d_grad", "traj_grad", "uneven"],
+    ap.add_argument("--case", default="", choices=["", "large", "traj3d", "traj3d_grad", "traj_grad", "uneven",
+                                                   "adjoint"],
                     help="run one small workload of the named kernel twice and exit (profiling runs)")
     ap.add_argument("--traj3d-full", type=int, default=0, metavar="STEPS",
                     help="instead of the force maps: run the whole 3D ensemble (65,536 particles, "

@@ -6,9 +6,12 @@
 // the set's beams into shared memory and compacts the active
 // (ground, beam, excited) triples; then its threads stream over the set's
 // points.
-//  * Plain FP64 form (force_kernel, force_adjoint_kernel, traj1d_kernel):
-//    groups of G = 4 lanes per point, the reference's elimination
-//    (rate_core.cuh); the trajectory kernel runs a particle per group.
+//  * Plain FP64 form: the reference's elimination (rate_core.cuh).  Force
+//    maps (force_plain_kernel) and the adjoint (force_plain_adjoint_kernel):
+//    rates one point per thread into a shared table, then the elimination
+//    on groups of 2 (force) or 4 (adjoint, which keeps L) lanes per point,
+//    then (adjoint) the gradient passes one point per thread.  Trajectories
+//    (traj1d_kernel): a particle per group of G = 4 lanes (solve_point).
 //  * FP32-bulk and FP64-reduced forms (force_reduced_kernel,
 //    traj1d_reduced_kernel): one point or particle per thread (two points
 //    per thread for FP32 force maps without populations), populations from
@@ -24,127 +27,365 @@ namespace {
 
 constexpr int kThreads = 128;
 
-template <int NGMAX, int NEMAX, int G, bool EXACT>
-__global__ void __launch_bounds__(kThreads, 3)
-force_kernel(ForceParams P)
+// Plain FP64 force maps in two phases per round of TH points (one per thread):
+//  1. each thread computes its point's saturated rates R[g,e] and force terms
+//     F_g (reduced_rates<F64>: the reference's detuning chain and products,
+//     rate_equations_jit.py:58-90; the triples of a ground state run excited-
+//     state-major, beams ascending, so R[g,e] has the reference's summation
+//     order and F_g, s_g differ from it in rounding only) into a shared table;
+//  2. groups of G lanes solve the TH points' population systems from the
+//     table (group_factor: the reference's elimination with partial
+//     pivoting, without keeping L), TH / G points at a time; lane t builds
+//     its columns k = c*G + t of M' straight from the table.
+// Every record of the triple table is read by all threads at once
+// (broadcast), and the rates need no lane-to-lane exchange.  Rate table: per
+// ground state k, R[k][e] for e < NEMAX and F_k, each a row of TH doubles (a
+// thread's point in column p); rows of consecutive k sit 8 doubles apart
+// modulo 16, so the lanes of a group reading consecutive k of the same
+// point, 32 / G groups at once, take the minimum two wavefronts.
+// G = 2 (kPlainG): 6 columns per lane for SrOH.  Against 4 lanes per point
+// it halves the work every lane repeats for its group (multipliers, pivot
+// tests, shuffles); on 1024 SrOH sets x 256 x 256 it took 38.8 ms against
+// 54.8 ms at G = 4 and 75.7 ms for the former one-pass kernel (4 lanes per
+// point computing rates and elimination together).
+template <int NGMAX, int NEMAX, bool EXACT, int PAD, int TH, int G>
+__global__ void __launch_bounds__(TH, (TH <= 64 ? 4 : 2))
+force_plain_kernel(ForceParams P)
 {
     using GS = GroupShape<NGMAX, NEMAX, G>;
+    constexpr int CPL = GS::CPL;
+    constexpr int RBS = (NEMAX + 1) * TH + 8;
+    static_assert(((NEMAX + 1) * TH) % 16 == 0, "rate-table rows 8 doubles off a 16-double multiple");
     extern __shared__ __align__(16) unsigned char sm[];
-    SmemLayout Ly;
-    const int ngroups = kThreads / G;
-    Ly.build(P.n_g, P.n_e, P.n_b, GS::CPL, ngroups);
+    RedLayout<NGMAX, NEMAX> Ly;
+    Ly.build(P.n_b);
+    double *fds = (double *)(sm + Ly.total);   // [n_b][TH]: Doppler-shifted beam frequencies
+    double *rtab = fds + (size_t)P.n_b * TH;   // [NGMAX][RBS]
+    const int tid = threadIdx.x, lane = tid & 31, t = lane % G, gbase = lane - t, group = tid / G;
+    const int n_g = EXACT ? NGMAX : P.n_g;
+    const int n_e = EXACT ? NEMAX : P.n_e;
+    const double gh2 = (P.Gamma / 2.0) * (P.Gamma / 2.0);
     const long long pts_per_set = (P.layout == MM_LAYOUT_GRID) ? P.nv * P.nz : P.pps;
-
-    const int lane = threadIdx.x & 31, t = lane % G, gbase = lane - t;
-    const int group = threadIdx.x / G;
-    double *scr = (double *)(sm + Ly.scratch) + (size_t)group * Ly.scratch_per_group;
-    double *fd = scr, *Ese = scr + P.n_b;
-
     for (int set = blockIdx.y; set < P.n_sets; set += gridDim.y) {
         const long long set_first = (long long)set * pts_per_set;
         long long set_count = pts_per_set;
         if (set_first + set_count > P.n_points) set_count = P.n_points - set_first;
         if (set_count <= 0) continue;  // uniform over the CTA
-        SetView S;
+        RedView S;
         __syncthreads();
-        build_set_tables<G, GS::CPL>(P, set, sm, Ly, S);
+        build_reduced_tables<NGMAX, NEMAX, PAD, true>(P, set, sm, Ly, S);
         const double Bg = P.bgrad[set];
         const long long chunk = (set_count + gridDim.x - 1) / gridDim.x;
         const long long start = (long long)blockIdx.x * chunk;
         const long long end = min(start + chunk, set_count);
-        for (long long base = start; base < end; base += ngroups) {
-            const long long ip = base + group;
-            const bool valid = ip < end;
-            const long long ipc = valid ? ip : start;
-            double v, z;
-            if (P.layout == MM_LAYOUT_GRID) {
-                v = P.v[ipc / P.nz];
-                z = P.z[ipc % P.nz];
-            } else {
-                v = P.v[set_first + ipc];
-                z = P.z[set_first + ipc];
-            }
-            double xs[GS::CPL];
-            const PointOut o = solve_point<NGMAX, NEMAX, G, EXACT>(P, S, fd, Ese, t, gbase, v, z, Bg, xs);
-            if (valid) {
-                const long long gi = set_first + ip;
-                if (t == 0) {
-                    P.F[gi] = o.F;
-                    if (P.R) P.R[gi] = o.R;
-                    if (P.status) P.status[gi] = o.status;
+        for (long long base = start; base < end; base += TH) {
+            // ---- phase 1: rates of point base + tid ----
+            if (base + tid < end) {
+                const long long ip = base + tid;
+                double v, z;
+                if (P.layout == MM_LAYOUT_GRID) {
+                    v = P.v[ip / P.nz];
+                    z = P.z[ip % P.nz];
+                } else {
+                    v = P.v[set_first + ip];
+                    z = P.z[set_first + ip];
                 }
-                if (P.pop) {
+                RateCtx<NEMAX> C;
+                C.B = __dmul_rn(__dmul_rn(Bg, z), 1e4);
+                C.vf = 0.0f;
+                C.Bf = 0.0f;
+                C.fd = fds + tid;
+                C.stride = TH;
+                for (int b = 0; b < P.n_b; b++)
+                    fds[b * TH + tid] = __dadd_rn(S.freq[b], __ddiv_rn(__dmul_rn(S.ck[b], v), MM_TWO_PI));
 #pragma unroll
-                    for (int c = 0; c < GS::CPL; c++) {
-                        const int k = c * G + t;
-                        if (k < P.n_g) P.pop[gi * P.n_g + k] = xs[c];
+                for (int e = 0; e < NEMAX; e++)
+                    C.Ese[e] = (e < n_e) ? __dadd_rn(S.E[n_g + e],
+                                                     __ddiv_rn(__dmul_rn(__dmul_rn(C.B, S.zde[e]), P.Gamma), MM_TWO_PI))
+                                         : 0.0;
+                for (int g = 0; g < n_g; g++) {
+                    double Re[NEMAX], f, s;
+                    reduced_rates<NEMAX, PAD, true>(S, g, C, gh2, Re, f, s);
+                    // saturation correction 1/(1 + s_total[g]) (rate_equations_jit.py:85-90)
+                    const double sat = mm_rcp(1.0 + s);
+                    double *row = rtab + (size_t)g * RBS + tid;
+#pragma unroll
+                    for (int e = 0; e < NEMAX; e++) row[e * TH] = Re[e] * sat;
+                    row[NEMAX * TH] = f * sat;
+                }
+            }
+            __syncthreads();
+            // ---- phase 2: population systems, TH / G points per pass ----
+#pragma unroll 1
+            for (int q = 0; q < G; q++) {
+                const int p = q * (TH / G) + group;
+                const long long ip = base + p;
+                // warps whose points all lie beyond the chunk skip the pass (lanes of
+                // a partly filled warp solve whatever the table holds, unused)
+                if (!__any_sync(0xffffffffu, ip < end)) continue;
+                // columns of M' straight from the rate table (one column's rates live at a time)
+                double A[CPL][NGMAX], invU[CPL], xs[CPL];
+#pragma unroll
+                for (int c = 0; c < CPL; c++) {
+                    const int k = c * G + t;
+                    const bool own = EXACT ? (k < NGMAX) : (k < n_g);
+                    const double *row = rtab + (size_t)(own ? k : 0) * RBS + p;
+                    double Rc[NEMAX], rs = 0.0;
+#pragma unroll
+                    for (int e = 0; e < NEMAX; e++) {
+                        Rc[e] = own ? row[e * TH] : 0.0;
+                        rs += Rc[e];
+                    }
+#pragma unroll
+                    for (int r = 0; r < NGMAX; r++) {
+                        double br[NEMAX];
+#pragma unroll
+                        for (int e = 0; e < NEMAX; e++) br[e] = (r < n_g && e < n_e) ? S.brt[r * NEMAX + e] : 0.0;
+                        A[c][r] = mprime_entry<NGMAX, NEMAX, G, EXACT>(n_g, r, k, Rc, rs, br);
+                    }
+                }
+                int prows[NGMAX];
+                bool swapped;
+                int stat = 0;
+                group_factor<NGMAX, NEMAX, G, EXACT, false>(P, t, gbase, A, invU, prows, swapped, xs, stat);
+                double Rk[CPL], Fk[CPL];
+#pragma unroll
+                for (int c = 0; c < CPL; c++) {
+                    const int k = c * G + t;
+                    const bool own = EXACT ? (k < NGMAX) : (k < n_g);
+                    const double *row = rtab + (size_t)(own ? k : 0) * RBS + p;
+                    double rs = 0.0;
+#pragma unroll
+                    for (int e = 0; e < NEMAX; e++) rs += own ? row[e * TH] : 0.0;
+                    Rk[c] = rs;
+                    Fk[c] = own ? row[NEMAX * TH] : 0.0;
+                }
+                PointOut o = group_finish<NGMAX, NEMAX, G, EXACT>(P, t, xs, Fk, Rk, stat);
+                if (!isfinite(o.F)) stat |= MM_ST_NONFINITE;
+                o.status = mm_group_or(stat, G);
+                if (ip < end) {
+                    const long long gi = set_first + ip;
+                    if (t == 0) {
+                        P.F[gi] = o.F;
+                        if (P.R) P.R[gi] = o.R;
+                        if (P.status) P.status[gi] = o.status;
+                    }
+                    if (P.pop) {
+#pragma unroll
+                        for (int c = 0; c < CPL; c++) {
+                            const int k = c * G + t;
+                            if (k < P.n_g) P.pop[gi * P.n_g + k] = xs[c];
+                        }
                     }
                 }
             }
+            __syncthreads();  // the next round rewrites the rate table
         }
     }
 }
 
-// Forward force plus its gradient with respect to every beam's frequency and
-// s0 and the set's B' (implicit differentiation through the steady state;
-// the adjoint section of solve_point).  grad row layout per point:
-// [dF/dfreq_0 .. dF/dfreq_{nb-1}, dF/ds0_0 .. dF/ds0_{nb-1}, dF/dB'].
-template <int NGMAX, int NEMAX, int G, bool EXACT>
-__global__ void __launch_bounds__(kThreads, 2)
-force_adjoint_kernel(ForceParams P, double *grad)
+// The plain form's force and its gradient (implicit differentiation through
+// the steady state) in three phases per round of
+// TH points:
+//  1. one thread per point: saturated rates into the rate table, as
+//     force_plain_kernel, plus each ground state's saturation factor;
+//  2. groups of G lanes: the elimination keeping L (group_factor), the
+//     populations and force (group_finish), and the multipliers lambda and nu
+//     of the transposed solve (group_lambda); p_g and lambda_g replace the
+//     first two rate rows of the point's column, nu goes to its own table;
+//  3. one thread per point: the two passes over each ground state's triples
+//     (dF/dtheta = sum (p_g hk_b - mu[g,e]) d rate_bge / dtheta, with
+//     mu[g,e] = p_g (nu_e - lambda_g [g < n_g - 1])) into the thread's own
+//     accumulators (no atomics; a fixed summation order).
+// grad row layout per point: [dF/dfreq_0 .. dF/dfreq_{nb-1}, dF/ds0_0 ..
+// dF/ds0_{nb-1}, dF/dB'].
+template <int NGMAX, int NEMAX, bool EXACT, int PAD, int TH, int G>
+__global__ void __launch_bounds__(TH, 3)
+force_plain_adjoint_kernel(ForceParams P, double *grad)
 {
     using GS = GroupShape<NGMAX, NEMAX, G>;
+    constexpr int CPL = GS::CPL;
+    constexpr int RBS = (NEMAX + 2) * TH + 8;  // rows: R[k][e] sat, F_k sat, sat_k
+    static_assert(((NEMAX + 2) * TH) % 16 == 0, "rate-table rows 8 doubles off a 16-double multiple");
     extern __shared__ __align__(16) unsigned char sm[];
-    SmemLayout Ly;
-    const int ngroups = kThreads / G;
-    Ly.build(P.n_g, P.n_e, P.n_b, GS::CPL, ngroups);
-    const long long pts_per_set = (P.layout == MM_LAYOUT_GRID) ? P.nv * P.nz : P.pps;
-    const int lane = threadIdx.x & 31, t = lane % G, gbase = lane - t;
-    const int group = threadIdx.x / G;
-    double *scr = (double *)(sm + Ly.scratch) + (size_t)group * Ly.scratch_per_group;
-    double *fd = scr, *Ese = scr + P.n_b, *gacc = scr + P.n_b + P.n_e;
+    RedLayout<NGMAX, NEMAX> Ly;
+    Ly.build(P.n_b, true);
     const int nb = P.n_b, gw = 2 * nb + 1;
+    double *fds = (double *)(sm + Ly.total);      // [n_b][TH]
+    double *gas = fds + (size_t)nb * TH;          // [2 n_b][TH]: dF/dfreq_b, dF/ds0_b
+    double *nut = gas + (size_t)2 * nb * TH;      // [NEMAX][TH]
+    double *rtab = nut + (size_t)NEMAX * TH;      // [NGMAX][RBS]
+    const int tid = threadIdx.x, lane = tid & 31, t = lane % G, gbase = lane - t, group = tid / G;
+    const int n_g = EXACT ? NGMAX : P.n_g;
+    const int n_e = EXACT ? NEMAX : P.n_e;
+    const double gh = P.Gamma / 2.0, gh2 = gh * gh, geff = P.geff;
+    const long long pts_per_set = (P.layout == MM_LAYOUT_GRID) ? P.nv * P.nz : P.pps;
     for (int set = blockIdx.y; set < P.n_sets; set += gridDim.y) {
         const long long set_first = (long long)set * pts_per_set;
         long long set_count = pts_per_set;
         if (set_first + set_count > P.n_points) set_count = P.n_points - set_first;
-        if (set_count <= 0) continue;
-        SetView S;
+        if (set_count <= 0) continue;  // uniform over the CTA
+        RedView S;
         __syncthreads();
-        build_set_tables<G, GS::CPL>(P, set, sm, Ly, S);
+        build_reduced_tables<NGMAX, NEMAX, PAD, true>(P, set, sm, Ly, S);
         const double Bg = P.bgrad[set];
         const long long chunk = (set_count + gridDim.x - 1) / gridDim.x;
         const long long start = (long long)blockIdx.x * chunk;
         const long long end = min(start + chunk, set_count);
-        for (long long base = start; base < end; base += ngroups) {
-            const long long ip = base + group;
-            const bool valid = ip < end;
-            const long long ipc = valid ? ip : start;
-            double v, z;
-            if (P.layout == MM_LAYOUT_GRID) {
-                v = P.v[ipc / P.nz];
-                z = P.z[ipc % P.nz];
-            } else {
-                v = P.v[set_first + ipc];
-                z = P.z[set_first + ipc];
-            }
-            double xs[GS::CPL];
-            const PointOut o = solve_point<NGMAX, NEMAX, G, EXACT, true>(
-                P, S, fd, Ese, t, gbase, v, z, Bg, xs, gacc);
-            if (valid) {
-                const long long gi = set_first + ip;
-                if (t == 0) {
-                    P.F[gi] = o.F;
-                    if (P.R) P.R[gi] = o.R;
-                    if (P.status) P.status[gi] = o.status;
-                    grad[gi * gw + 2 * nb] = o.gB;
+        for (long long base = start; base < end; base += TH) {
+            const bool mine = base + tid < end;
+            double v = 0.0, z = 0.0;
+            RateCtx<NEMAX> C;
+            if (mine) {
+                const long long ip = base + tid;
+                if (P.layout == MM_LAYOUT_GRID) {
+                    v = P.v[ip / P.nz];
+                    z = P.z[ip % P.nz];
+                } else {
+                    v = P.v[set_first + ip];
+                    z = P.z[set_first + ip];
                 }
-                for (int i = t; i < 2 * nb; i += G) grad[gi * gw + i] = gacc[i];
             }
-            __syncwarp();
+            C.B = __dmul_rn(__dmul_rn(Bg, z), 1e4);
+            C.vf = 0.0f;
+            C.Bf = 0.0f;
+            C.fd = fds + tid;
+            C.stride = TH;
+#pragma unroll
+            for (int e = 0; e < NEMAX; e++)
+                C.Ese[e] = (e < n_e) ? __dadd_rn(S.E[n_g + e],
+                                                 __ddiv_rn(__dmul_rn(__dmul_rn(C.B, S.zde[e]), P.Gamma), MM_TWO_PI))
+                                     : 0.0;
+            // ---- phase 1: rates ----
+            if (mine) {
+                for (int b = 0; b < nb; b++)
+                    fds[b * TH + tid] = __dadd_rn(S.freq[b], __ddiv_rn(__dmul_rn(S.ck[b], v), MM_TWO_PI));
+                for (int g = 0; g < n_g; g++) {
+                    double Re[NEMAX], f, s;
+                    reduced_rates<NEMAX, PAD, true>(S, g, C, gh2, Re, f, s);
+                    const double sat = mm_rcp(1.0 + s);  // rate_equations_jit.py:85-90
+                    double *row = rtab + (size_t)g * RBS + tid;
+#pragma unroll
+                    for (int e = 0; e < NEMAX; e++) row[e * TH] = Re[e] * sat;
+                    row[NEMAX * TH] = f * sat;
+                    row[(NEMAX + 1) * TH] = sat;
+                }
+            }
+            __syncthreads();
+            // ---- phase 2: elimination, populations, multipliers ----
+#pragma unroll 1
+            for (int q = 0; q < G; q++) {
+                const int p = q * (TH / G) + group;
+                const long long ip = base + p;
+                if (!__any_sync(0xffffffffu, ip < end)) continue;
+                double A[CPL][NGMAX], invU[CPL], xs[CPL], Rk[CPL], Fk[CPL];
+#pragma unroll
+                for (int c = 0; c < CPL; c++) {
+                    const int k = c * G + t;
+                    const bool own = EXACT ? (k < NGMAX) : (k < n_g);
+                    const double *row = rtab + (size_t)(own ? k : 0) * RBS + p;
+                    double Rc[NEMAX], rs = 0.0;
+#pragma unroll
+                    for (int e = 0; e < NEMAX; e++) {
+                        Rc[e] = own ? row[e * TH] : 0.0;
+                        rs += Rc[e];
+                    }
+                    Rk[c] = rs;
+                    Fk[c] = own ? row[NEMAX * TH] : 0.0;
+#pragma unroll
+                    for (int r = 0; r < NGMAX; r++) {
+                        double br[NEMAX];
+#pragma unroll
+                        for (int e = 0; e < NEMAX; e++) br[e] = (r < n_g && e < n_e) ? S.brt[r * NEMAX + e] : 0.0;
+                        A[c][r] = mprime_entry<NGMAX, NEMAX, G, EXACT>(n_g, r, k, Rc, rs, br);
+                    }
+                }
+                int prows[NGMAX];
+                bool swapped;
+                int stat = 0;
+                group_factor<NGMAX, NEMAX, G, EXACT, true>(P, t, gbase, A, invU, prows, swapped, xs, stat);
+                PointOut o = group_finish<NGMAX, NEMAX, G, EXACT>(P, t, xs, Fk, Rk, stat);
+                double wv[NGMAX], nu[NEMAX];
+                group_lambda<NGMAX, NEMAX, G, EXACT>(P, S.brt, 1, NEMAX, t, gbase, A, invU, prows, swapped, Fk,
+                                                     wv, nu);
+                if (!isfinite(o.F)) stat |= MM_ST_NONFINITE;
+                o.status = mm_group_or(stat, G);
+                __syncwarp();
+                // p_g and lambda_g over the first two rate rows of the point (read above)
+#pragma unroll
+                for (int c = 0; c < CPL; c++) {
+                    const int k = c * G + t;
+                    if (EXACT ? (k < NGMAX) : (k < n_g)) {
+                        double *row = rtab + (size_t)k * RBS + p;
+                        double lam = 0.0;
+#pragma unroll
+                        for (int g = 0; g < NGMAX; g++)
+                            if (g == k) lam = wv[g];
+                        row[0] = xs[c];
+                        row[TH] = lam;
+                    }
+                }
+                if (t == 0) {
+#pragma unroll
+                    for (int e = 0; e < NEMAX; e++) nut[e * TH + p] = nu[e];
+                    if (ip < end) {
+                        const long long gi = set_first + ip;
+                        P.F[gi] = o.F;
+                        if (P.R) P.R[gi] = o.R;
+                        if (P.status) P.status[gi] = o.status;
+                    }
+                }
+            }
+            __syncthreads();
+            // ---- phase 3: gradient passes over the triples ----
+            if (mine) {
+                const long long gi = set_first + base + tid;
+                for (int i = 0; i < 2 * nb; i++) gas[i * TH + tid] = 0.0;
+                double nue[NEMAX];
+#pragma unroll
+                for (int e = 0; e < NEMAX; e++) nue[e] = nut[e * TH + tid];
+                double gB = 0.0;
+                for (int g = 0; g < n_g; g++) {
+                    const double *row = rtab + (size_t)g * RBS + tid;
+                    const double pk = row[0], lamk = row[TH], sat = row[(NEMAX + 1) * TH];
+                    const double Esg = fma(C.B, S.czd[g], S.E[g]);
+                    double T = 0.0;
+#pragma unroll 1
+                    for (int pass = 0; pass < 2; pass++) {
+                        const double Cs = T * sat;
+#pragma unroll
+                        for (int e = 0; e < NEMAX; e++) {
+                            const double mue = pk * (nue[e] - ((g < n_g - 1) ? lamk : 0.0));
+                            const double ddB = (e < n_e) ? -z * 1e4 * (P.zd[n_g + e] - P.zd[g]) * P.Gamma : 0.0;
+                            const int i1 = S.offs[g * NEMAX + e + 1];
+                            for (int i = S.offs[g * NEMAX + e]; i < i1; i++) {
+                                const TripD tr = ((const TripD *)S.trip)[i];
+                                const double om = __dsub_rn(C.Ese[e], Esg);
+                                const double de = __dmul_rn(__dsub_rn(fds[tr.b * TH + tid], om), MM_TWO_PI);
+                                const double L = gh2 * mm_rcp(fma(de, de, gh2));
+                                const double rate = tr.c1 * L * sat;
+                                const double w = pk * tr.hk - mue;
+                                if (pass == 0) {
+                                    T = fma(w, rate, T);
+                                } else {
+                                    const double Q = w * rate - Cs * tr.c2 * L;
+                                    const double dLL = -2.0 * de * L / gh2;  // (dL/d delta) / L
+                                    gas[tr.b * TH + tid] += Q * dLL * MM_TWO_PI;
+                                    gas[(nb + tr.b) * TH + tid] += S.d2t[i] * L * (w * gh * geff * sat - Cs);
+                                    gB = fma(Q * dLL, ddB, gB);
+                                }
+                            }
+                        }
+                    }
+                }
+                for (int i = 0; i < 2 * nb; i++) grad[gi * gw + i] = gas[i * TH + tid];
+                grad[gi * gw + 2 * nb] = gB;
+            }
+            __syncthreads();  // the next round rewrites the tables
         }
     }
 }
+
 
 // FP32-bulk form: one point per thread, populations from the reduced
 // (excited-manifold) solve of reduced.cuh.  One CTA per parameter set at a
@@ -253,7 +494,7 @@ force_reduced_kernel(ForceParams P)
 }
 
 // FP64-reduced adjoint: the FP64-reduced force and its gradient (same row
-// layout as force_adjoint_kernel), one point per thread.  The host launches it
+// layout as force_plain_adjoint_kernel), one point per thread.  The host launches it
 // only when every set passes the reduced form's structural checks.  Shared
 // scratch per thread: Doppler-shifted frequencies, dF/dfreq_b and dF/ds0_b
 // (3 n_b doubles, stride blockDim.x).
@@ -681,33 +922,34 @@ size_t smem_bytes(const ForceParams &P)
     return Ly.total;
 }
 
-template <class C>
-int launch_force(const ForceParams &P, long long pts_per_set, cudaStream_t st)
+constexpr int kPlainThreads = 64;
+constexpr int kPlainG = 2;  // lanes per point in the elimination
+
+template <class C, int PAD>
+int launch_plain(const ForceParams &P, long long pts_per_set, cudaStream_t st)
 {
-    auto kern = force_kernel<C::ng, C::ne, C::g, C::exact>;
-    const size_t sb = smem_bytes<C>(P);
+    constexpr int TH = kPlainThreads;
+    auto kern = force_plain_kernel<C::ng, C::ne, C::exact, PAD, TH, kPlainG>;
+    RedLayout<C::ng, C::ne> Ly;
+    Ly.build(P.n_b);
+    const size_t sb = Ly.total + sizeof(double) * ((size_t)P.n_b * TH + (size_t)C::ng * ((C::ne + 1) * TH + 8));
     if (sb > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb);
         if (mm_cuda_check(e, "cudaFuncSetAttribute")) return -3;
     }
-    int dev = 0, nsm = 148;
+    int dev = 0, nsm = 148, per_sm = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    int per_sm = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, sb);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, TH, sb);
     if (per_sm < 1) per_sm = 1;
-    const int ngroups = kThreads / C::g;
-    // enough CTAs per set to fill the GPU a few times over, at least 64 points per group
+    // enough CTAs to fill the GPU a few times over, at least 8 rounds of TH points each
     const long long want = (long long)nsm * per_sm * 4;
     long long gx = std::max<long long>(1, want / std::max(1, P.n_sets));
-    const long long max_gx = std::max<long long>(1, (pts_per_set + (long long)ngroups * 64 - 1) /
-                                                      ((long long)ngroups * 64));
-    gx = std::min(gx, max_gx);
+    gx = std::min(gx, std::max<long long>(1, (pts_per_set + TH * 8 - 1) / (TH * 8)));
     gx = std::min<long long>(gx, 1 << 20);
-    const int gy = std::min(P.n_sets, 65535);
-    dim3 grid((unsigned)gx, (unsigned)gy);
-    kern<<<grid, kThreads, sb, st>>>(P);
-    return mm_cuda_check(cudaGetLastError(), "force_kernel launch") ? -3 : 0;
+    dim3 grid((unsigned)gx, (unsigned)std::min(P.n_sets, 65535));
+    kern<<<grid, TH, sb, st>>>(P);
+    return mm_cuda_check(cudaGetLastError(), "force_plain_kernel launch") ? -3 : 0;
 }
 
 template <class C, int PAD, bool F64>
@@ -752,11 +994,19 @@ int launch_traj_reduced(const ForceParams &P, const TrajParams &T, cudaStream_t 
     return mm_cuda_check(cudaGetLastError(), "traj1d_reduced_kernel launch") ? -3 : 0;
 }
 
-template <class C>
-int launch_adjoint(const ForceParams &P, double *grad, cudaStream_t st)
+
+constexpr int kPlainAdjThreads = 64;
+constexpr int kPlainAdjG = 4;
+
+template <class C, int PAD>
+int launch_plain_adjoint(const ForceParams &P, double *grad, cudaStream_t st)
 {
-    auto kern = force_adjoint_kernel<C::ng, C::ne, C::g, C::exact>;
-    const size_t sb = smem_bytes<C>(P);
+    constexpr int TH = kPlainAdjThreads;
+    auto kern = force_plain_adjoint_kernel<C::ng, C::ne, C::exact, PAD, TH, kPlainAdjG>;
+    RedLayout<C::ng, C::ne> Ly;
+    Ly.build(P.n_b, true);
+    const size_t sb = Ly.total + sizeof(double) * ((size_t)3 * P.n_b * TH + (size_t)C::ne * TH +
+                                                   (size_t)C::ng * ((C::ne + 2) * TH + 8));
     if (sb > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb);
         if (mm_cuda_check(e, "cudaFuncSetAttribute")) return -3;
@@ -764,16 +1014,16 @@ int launch_adjoint(const ForceParams &P, double *grad, cudaStream_t st)
     int dev = 0, nsm = 148, per_sm = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, sb);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, TH, sb);
     if (per_sm < 1) per_sm = 1;
-    const int ngroups = kThreads / C::g;
     const long long pts_per_set = (P.layout == MM_LAYOUT_GRID) ? P.nv * P.nz : P.pps;
     const long long want = (long long)nsm * per_sm * 4;
     long long gx = std::max<long long>(1, want / std::max(1, P.n_sets));
-    gx = std::min(gx, std::max<long long>(1, (pts_per_set + ngroups - 1) / ngroups));
+    gx = std::min(gx, std::max<long long>(1, (pts_per_set + TH * 4 - 1) / (TH * 4)));
+    gx = std::min<long long>(gx, 1 << 20);
     dim3 grid((unsigned)gx, (unsigned)std::min(P.n_sets, 65535));
-    kern<<<grid, kThreads, sb, st>>>(P, grad);
-    return mm_cuda_check(cudaGetLastError(), "force_adjoint_kernel launch") ? -3 : 0;
+    kern<<<grid, TH, sb, st>>>(P, grad);
+    return mm_cuda_check(cudaGetLastError(), "force_plain_adjoint_kernel launch") ? -3 : 0;
 }
 
 template <class C, int PAD>
@@ -959,9 +1209,9 @@ extern "C" int mm_force_adjoint(const mm_pack *pack, const mm_beams *beams, cons
     const bool red = opts->precision == MM_PREC_FP64_REDUCED && reduced_all_valid(pack, beams);
     return dispatch_class(P.n_g, P.n_e, [&](auto C) -> int {
         using CT = decltype(C);
-        if (!red) return launch_adjoint<CT>(P, grad, st);
-        return reduced_list_granule(pack, beams) == kRedPad ? launch_reduced_adjoint<CT, kRedPad>(P, grad, st)
-                                                             : launch_reduced_adjoint<CT, 1>(P, grad, st);
+        const bool pad = reduced_list_granule(pack, beams) == kRedPad;
+        if (!red) return pad ? launch_plain_adjoint<CT, kRedPad>(P, grad, st) : launch_plain_adjoint<CT, 1>(P, grad, st);
+        return pad ? launch_reduced_adjoint<CT, kRedPad>(P, grad, st) : launch_reduced_adjoint<CT, 1>(P, grad, st);
     });
 }
 
@@ -1026,8 +1276,8 @@ extern "C" int mm_force_batch(const mm_pack *pack, const mm_beams *beams, const 
         return mm_large_force(P, pps, prec != MM_PREC_FP64 && reduced_all_valid(pack, beams), st);
     return dispatch_class(P.n_g, P.n_e, [&](auto C) -> int {
         using CT = decltype(C);
-        if (prec == MM_PREC_FP64) return launch_force<CT>(P, pps, st);
         const bool pad = reduced_list_granule(pack, beams) == kRedPad;
+        if (prec == MM_PREC_FP64) return pad ? launch_plain<CT, kRedPad>(P, pps, st) : launch_plain<CT, 1>(P, pps, st);
         if (prec == MM_PREC_FP64_REDUCED)
             return pad ? launch_reduced<CT, kRedPad, true>(P, pps, st) : launch_reduced<CT, 1, true>(P, pps, st);
         return pad ? launch_reduced<CT, kRedPad, false>(P, pps, st) : launch_reduced<CT, 1, false>(P, pps, st);

@@ -13,8 +13,8 @@
 //  2. Eigen-decomposition of the complex Hermitian H in shared memory
 //     (hermitian_eigen): Householder reduction to tridiagonal form (a lane per
 //     row), a phase change to a real tridiagonal matrix and implicit QL
-//     iterations that every lane runs on its own copy, rotating its own row
-//     of the eigenvector matrix.  Eigenvalues are sorted ascending with their
+//     iterations whose scalar recurrences every lane runs on shuffled values,
+//     rotating its own row of the eigenvector matrix.  Eigenvalues are sorted ascending with their
 //     vectors, as numpy.linalg.eigh returns them; Es_g[i] = E_g[i] + lambda_i.
 //  3. |U^H |tdm||^2 per (eigenstate, e, q); branching ratios.
 //  4. Lane g accumulates, over beams and excited states, the unsaturated rates,
@@ -162,9 +162,9 @@ struct Keep3 {
 //    P = I - 2 v v^H (|v| = 1) maps H[k+1 .., k] to (alpha, 0, ..),
 //    alpha = -e^{i arg H[k+1][k]} |H[k+1 .., k]|; the trailing block becomes
 //    H - 2 v w^H - 2 w v^H with w = p - (v^H p) v, p = H v, and Q <- Q P.
-//  * QL: every lane runs the same scalar recurrences on its own copy of the
-//    diagonal d and off-diagonal e and applies each rotation to its own row
-//    of Z, so the lanes need no communication in this phase.
+//  * QL: lane i holds d_i and e_i; every lane runs the same scalar
+//    recurrences on values fetched by shuffles and applies each rotation to
+//    its own row of Z (in shared memory).
 template <int NGM, class GroupT>
 __device__ bool hermitian_eigen(GroupT &W, int t, int n)
 {
@@ -240,21 +240,20 @@ __device__ bool hermitian_eigen(GroupT &W, int t, int n)
         }
         __syncwarp();
     }
-    // real symmetric tridiagonal: d_i = H[i][i], e_i = |H[i+1][i]|, phases
-    // delta_0 = 1, delta_{i+1} = delta_i H[i+1][i] / |H[i+1][i]|
-    double d[NGM], e[NGM], dr[NGM], di[NGM], z[NGM];
+    // real symmetric tridiagonal: lane i holds d_i = H[i][i] and
+    // e_i = |H[i+1][i]| in registers; phases delta_0 = 1,
+    // delta_{i+1} = delta_i H[i+1][i] / |H[i+1][i]|
+    double dr[NGM], di[NGM];
+    double dl = (row) ? W.Hre[t * LDH + t] : 0.0, el = 0.0;
     double cr = 1.0, ci = 0.0;
 #pragma unroll
     for (int i = 0; i < NGM; i++) {
-        d[i] = (i < n) ? W.Hre[i * LDH + i] : 0.0;
         dr[i] = cr;
         di[i] = ci;
-        e[i] = 0.0;
-        z[i] = (i == t) ? 1.0 : 0.0;
         if (i + 1 < n) {
             const double hr = W.Hre[(i + 1) * LDH + i], hi = W.Him[(i + 1) * LDH + i];
             const double a = sqrt(hr * hr + hi * hi);
-            e[i] = a;
+            if (i == t) el = a;
             if (a > 0.0) {
                 const double ur = hr / a, ui = hi / a;
                 const double nr = cr * ur - ci * ui;
@@ -263,53 +262,70 @@ __device__ bool hermitian_eigen(GroupT &W, int t, int n)
             }
         }
     }
-    // implicit QL with Wilkinson shifts; lane t applies the rotations to row t of Z
+    __syncwarp();
+    // row t of the rotation product Z, kept in row t of Hre (H is no longer needed)
+    double *z = W.Hre + (row ? t : 0) * LDH;
+    if (row)
+        for (int j = 0; j < n; j++) z[j] = (j == t) ? 1.0 : 0.0;
+    // implicit QL with Wilkinson shifts.  The recurrences run on every lane of
+    // the group with d_i, e_i fetched from lane i by shuffles (an index of a
+    // register array that is only known at run time would put the array in
+    // local memory); lane i + 1 updates its own d, e; lane t applies each
+    // rotation to its row of Z.  All control flow is uniform over the group
+    // (it depends only on shuffled values), and the two groups of a warp may
+    // take different paths: the shuffles name this group's 16 lanes only.
+    const unsigned gmask = 0xffffu << (threadIdx.x & 16);
     bool ok = true;
     for (int l = 0; l < n; l++) {
         for (int iter = 0;; iter++) {
-            int m = l;
-            for (; m + 1 < n; m++) {
-                const double dd = fabs(d[m]) + fabs(d[m + 1]);
-                if (fabs(e[m]) <= 2.220446049250313e-16 * dd) break;
-            }
+            // m = the first index >= l with a negligible e_m (n - 1 if none)
+            const double dn = __shfl_down_sync(gmask, dl, 1, 16);
+            const bool small = (t + 1 < n) && t >= l &&
+                               fabs(el) <= 2.220446049250313e-16 * (fabs(dl) + fabs(dn));
+            const unsigned bal = (__ballot_sync(gmask, small) >> (threadIdx.x & 16)) & 0xffffu;
+            const int m = bal ? __ffs(bal) - 1 : n - 1;
             if (m == l) break;
             if (iter == 60) { ok = false; break; }
-            double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
+            const double d_l = __shfl_sync(gmask, dl, l, 16), d_l1 = __shfl_sync(gmask, dl, l + 1, 16);
+            const double e_l = __shfl_sync(gmask, el, l, 16), d_m = __shfl_sync(gmask, dl, m, 16);
+            double g = (d_l1 - d_l) / (2.0 * e_l);
             double r = sqrt(fma(g, g, 1.0));
-            g = d[m] - d[l] + e[l] / (g + copysign(r, g));
+            g = d_m - d_l + e_l / (g + copysign(r, g));
             double s = 1.0, c = 1.0, p = 0.0;
-            int i = m - 1;
-            for (; i >= l; i--) {
-                const double f = s * e[i], b = c * e[i];
+            double dnext = d_m;  // d_{i+1} before this sweep
+            bool defl = false;
+            for (int i = m - 1; i >= l; i--) {
+                const double ei = __shfl_sync(gmask, el, i, 16), dii = __shfl_sync(gmask, dl, i, 16);
+                const double f = s * ei, b = c * ei;
                 r = sqrt(fma(f, f, g * g));
-                e[i + 1] = r;
+                if (t == i + 1) el = r;
                 if (r == 0.0) {  // deflation: the rotation vanished
-                    d[i + 1] -= p;
-                    e[m] = 0.0;
+                    if (t == i + 1) dl -= p;
+                    if (t == m) el = 0.0;
+                    defl = true;
                     break;
                 }
                 s = f / r;
                 c = g / r;
-                g = d[i + 1] - p;
-                r = (d[i] - g) * s + 2.0 * c * b;
+                g = dnext - p;
+                r = (dii - g) * s + 2.0 * c * b;
                 p = s * r;
-                d[i + 1] = g + p;
+                if (t == i + 1) dl = g + p;
                 g = c * r - b;
-                const double z1 = z[i + 1];
-                z[i + 1] = fma(s, z[i], c * z1);
-                z[i] = fma(c, z[i], -s * z1);
+                if (row) {
+                    const double z1 = z[i + 1], z0 = z[i];
+                    z[i + 1] = fma(s, z0, c * z1);
+                    z[i] = fma(c, z0, -s * z1);
+                }
+                dnext = dii;
             }
-            if (r == 0.0 && i >= l) continue;
-            d[l] -= p;
-            e[l] = g;
-            e[m] = 0.0;
+            if (defl) continue;
+            if (t == l) { dl -= p; el = g; }
+            if (t == m) el = 0.0;
         }
     }
     __syncwarp();
-    // Z rows to shared memory (over H, no longer needed), then V <- Q D Z
-    if (row)
-        for (int j = 0; j < n; j++) W.Hre[t * LDH + j] = z[j];
-    __syncwarp();
+    // V <- Q D Z (Z rows in Hre)
     if (row) {
         double qr[NGM], qi[NGM];
 #pragma unroll
@@ -330,12 +346,16 @@ __device__ bool hermitian_eigen(GroupT &W, int t, int n)
             W.Vre[t * LDH + j] = ar;
             W.Vim[t * LDH + j] = ai;
         }
-        // ascending order (ties by index)
-        int rank = 0;
-        const double lt = d[t];
-        for (int j = 0; j < n; j++) rank += (d[j] < lt || (d[j] == lt && j < t)) ? 1 : 0;
+    }
+    // ascending order (ties by index); n is the same on both groups of the warp
+    int rank = 0;
+    for (int j = 0; j < n; j++) {
+        const double dj = __shfl_sync(0xffffffffu, dl, j, 16);
+        rank += (dj < dl || (dj == dl && j < t)) ? 1 : 0;
+    }
+    if (row) {
         W.perm[rank] = t;
-        W.lam[rank] = lt;
+        W.lam[rank] = dl;
     }
     __syncwarp();
     return ok;
@@ -397,7 +417,9 @@ __device__ Out3 force3d_point(const Force3Params &P, Smem3<NGM, NEM, TH> &S,
     for (int e = 0; e < NEM; e++) rowsum[e] = 0.0;
     if (t < n_g) {
         const int col = W.perm[t];
-        for (int e = 0; e < n_e; e++) {
+#pragma unroll
+        for (int e = 0; e < NEM; e++) {
+            if (e >= n_e) continue;
             for (int q = 0; q < 3; q++) {
                 double ar = 0.0, ai = 0.0;
                 for (int g = 0; g < n_g; g++) {
@@ -515,8 +537,10 @@ __device__ Out3 force3d_point(const Force3Params &P, Smem3<NGM, NEM, TH> &S,
         bv[i] = (i == n_g - 1) ? 1.0 : 0.0;
     }
     double invd = 0.0;
-#pragma unroll
-    for (int col = 0; col < NGM; col++) {
+    // static_for keeps every index of A and bv a compile-time constant (a
+    // plain unrolled loop left them in local memory in one size class)
+    static_for<0, NGM>([&](auto colc) {
+        constexpr int col = decltype(colc)::value;
         if (col < n_g) {
             int prow = col;
             if (t == col) {
@@ -553,16 +577,16 @@ __device__ Out3 force3d_point(const Force3Params &P, Smem3<NGM, NEM, TH> &S,
                 }
             }
         }
-    }
+    });
     double x = 0.0;
-#pragma unroll
-    for (int i = NGM - 1; i >= 0; i--) {
+    static_for<0, NGM>([&](auto iic) {
+        constexpr int i = NGM - 1 - decltype(iic)::value;
         if (i < n_g) {
             double part = (t > i && t < n_g) ? A[i] * x : 0.0;
             part = gsum16(part);
             if (t == i) x = (bv[i] - part) * invd;
         }
-    }
+    });
     if (kp) {
         kp->xraw = (t < n_g) ? x : 0.0;
 #pragma unroll
@@ -982,28 +1006,29 @@ __device__ void force3d_tangent(const Force3Params &P, const Tg3Params &T, Smem3
             rhs[i] = -gsum16(c);
         }
         // P M = L U with the forward's interchanges and factors (later interchanges
-        // were applied to the stored L columns, so all of P goes first)
-#pragma unroll
-        for (int col = 0; col < NGM; col++) {
+        // were applied to the stored L columns, so all of P goes first); static_for
+        // keeps the indices of rhs and xs compile-time constants (registers)
+        static_for<0, NGM>([&](auto colc) {
+            constexpr int col = decltype(colc)::value;
             if (col < n_g) {
                 const int pr = kp.prow[col];
 #pragma unroll
                 for (int rr = col + 1; rr < NGM; rr++)
                     if (rr == pr) { const double x = rhs[col]; rhs[col] = rhs[rr]; rhs[rr] = x; }
             }
-        }
-#pragma unroll
-        for (int col = 0; col < NGM; col++) {
+        });
+        static_for<0, NGM>([&](auto colc) {
+            constexpr int col = decltype(colc)::value;
             if (col < n_g) {
                 const double iv = TW.invd[col];
 #pragma unroll
                 for (int rr = col + 1; rr < NGM; rr++)
                     if (rr < n_g) rhs[rr] = fma(-(TW.LU[rr][col] * iv), rhs[col], rhs[rr]);
             }
-        }
+        });
         double dx = 0.0, xs[NGM];
-#pragma unroll
-        for (int i = NGM - 1; i >= 0; i--) {
+        static_for<0, NGM>([&](auto iic) {
+            constexpr int i = NGM - 1 - decltype(iic)::value;
             double xi = 0.0;
             if (i < n_g) {
                 double part = 0.0;
@@ -1014,7 +1039,7 @@ __device__ void force3d_tangent(const Force3Params &P, const Tg3Params &T, Smem3
             }
             xs[i] = xi;
             if (i == t) dx = xi;
-        }
+        });
         // clamp and normalisation
         double dxc = (lane && kp.xraw > 0.0) ? dx : 0.0;
         const double dtot = gsum16(dxc);

@@ -98,12 +98,11 @@ struct SetView {
     const double *freq, *ck;          // per beam: freq, (-k) kdir
     const int *cnt, *off, *maxcnt;    // per ground state / per slot
     const Trip64 *t64;
-    const double *d2t;                // |d|^2 of each FP64 triple (adjoint)
 };
 
 // Byte layout of the dynamic shared memory of the 1D force kernels.
 struct SmemLayout {
-    size_t E, zd, czd, BR, freq, ck, cnt, off, maxcnt, trip, d2t, scratch, total;
+    size_t E, zd, czd, BR, freq, ck, cnt, off, maxcnt, trip, scratch, total;
     int ntrip_max, scratch_per_group;  // doubles per group
 
     __host__ __device__ static size_t al(size_t x) { return (x + 15) & ~size_t(15); }
@@ -125,10 +124,9 @@ struct SmemLayout {
         // the 4 lanes of a group read records in different banks
         ntrip_max = n_g * n_b * n_e + 3 * n_g;
         trip = o; o = al(o + sizeof(Trip64) * (size_t)ntrip_max);
-        d2t = o; o = al(o + sizeof(double) * (size_t)ntrip_max);
-        // doppler-shifted frequencies, excited energies, adjoint accumulators
+        // per group: doppler-shifted frequencies and excited energies;
         // a stride of 2 (mod 4) doubles puts the 8 groups of a warp in distinct banks
-        scratch_per_group = ((n_b + n_e + 2 * n_b + 1) / 4) * 4 + 2;
+        scratch_per_group = ((n_b + n_e + 3) / 4) * 4 + 2;
         scratch = o; o = al(o + sizeof(double) * (size_t)scratch_per_group * ngroups);
         total = o;
     }
@@ -145,7 +143,6 @@ __device__ void build_set_tables(const ForceParams &P, int set, unsigned char *s
     double *freq = (double *)(sm + Ly.freq), *ck = (double *)(sm + Ly.ck);
     int *cnt = (int *)(sm + Ly.cnt), *off = (int *)(sm + Ly.off), *maxcnt = (int *)(sm + Ly.maxcnt);
     Trip64 *t64 = (Trip64 *)(sm + Ly.trip);
-    double *d2t = (double *)(sm + Ly.d2t);
     const int tid = threadIdx.x, nt = blockDim.x;
     const double *kdir = P.kdir + (size_t)set * n_b, *fr = P.freq + (size_t)set * n_b;
     const double *s0 = P.s0 + (size_t)set * n_b;
@@ -190,9 +187,12 @@ __device__ void build_set_tables(const ForceParams &P, int set, unsigned char *s
     const double gh = P.Gamma / 2.0;
     for (int k = tid; k < n_g; k += nt) {
         int o = off[k];
-        // order (b ascending, e ascending) = the reference's accumulation order
-        for (int b = 0; b < n_b; b++)
-            for (int e = 0; e < n_e; e++) {
+        // excited-state major, beams ascending: R[g,e] sums over b in the
+        // reference's order, and the force and saturation sums of g follow the
+        // order of the plain force maps (force_plain_kernel), so every plain-form
+        // kernel gives the same bits for the same point
+        for (int e = 0; e < n_e; e++)
+            for (int b = 0; b < n_b; b++) {
                 const double d2 = P.d2[(k * n_e + e) * 3 + pol[b]];
                 if (d2 < 1e-15) continue;
                 const double c1 = __dmul_rn(__dmul_rn(gh, s0[b]), d2);
@@ -203,13 +203,12 @@ __device__ void build_set_tables(const ForceParams &P, int set, unsigned char *s
                 tr.hk = hk;
                 tr.be = b | (e << 8);
                 tr.pad = 0;
-                d2t[o] = d2;
                 t64[o++] = tr;
             }
     }
     __syncthreads();
     S.E = E; S.zd = zd; S.czd = czd; S.BR = BR; S.freq = freq; S.ck = ck;
-    S.cnt = cnt; S.off = off; S.maxcnt = maxcnt; S.t64 = t64; S.d2t = d2t;
+    S.cnt = cnt; S.off = off; S.maxcnt = maxcnt; S.t64 = t64;
 }
 
 // Result of one point, identical in every lane of the group.
@@ -224,19 +223,326 @@ struct GroupShape {
     static constexpr int CPL = (NGMAX + G - 1) / G;  // column slots per lane
 };
 
+// One element of M' (lane t's column slot c holds column j = c*G + t): the
+// same operations wherever the matrix is built, so every caller gets the same
+// bits.  br[e] = BR[e, r].
+template <int NGMAX, int NEMAX, int G, bool EXACT>
+__device__ __forceinline__ double mprime_entry(int n_g, int r, int j, const double (&Rc)[NEMAX], double Rkc,
+                                               const double (&br)[NEMAX])
+{
+    double a;
+    if (EXACT || j < n_g) {
+        a = (r == j) ? -Rkc : 0.0;
+#pragma unroll
+        for (int e = 0; e < NEMAX; e++) a = fma(Rc[e], br[e], a);
+        if (r == n_g - 1) a = 1.0;           // normalisation row
+        if (!EXACT && r >= n_g) a = 0.0;
+    } else {
+        a = (r == j) ? 1.0 : 0.0;            // identity padding beyond n_g
+    }
+    return a;
+}
+
+// Columns of M' for the group's lanes from the saturated rates (row-major
+// pass; BR[e,r] read at BR[e * se + r * sr]).
+template <int NGMAX, int NEMAX, int G, bool EXACT>
+__device__ __forceinline__ void group_build(const ForceParams &P, const double *BR, int se, int sr, int t,
+                                            const double (&R)[GroupShape<NGMAX, NEMAX, G>::CPL][NEMAX],
+                                            const double (&Rk)[GroupShape<NGMAX, NEMAX, G>::CPL],
+                                            double (&A)[GroupShape<NGMAX, NEMAX, G>::CPL][NGMAX])
+{
+    constexpr int CPL = GroupShape<NGMAX, NEMAX, G>::CPL;
+    const int n_g = EXACT ? NGMAX : P.n_g;
+    const int n_e = EXACT ? NEMAX : P.n_e;
+#pragma unroll
+    for (int r = 0; r < NGMAX; r++) {
+        double br[NEMAX];
+#pragma unroll
+        for (int e = 0; e < NEMAX; e++) br[e] = (r < n_g && e < n_e) ? BR[e * se + r * sr] : 0.0;
+#pragma unroll
+        for (int c = 0; c < CPL; c++) A[c][r] = mprime_entry<NGMAX, NEMAX, G, EXACT>(n_g, r, c * G + t, R[c], Rk[c], br);
+    }
+}
+
+// Population system of one point from its saturated rates (the part of the
+// solve after the rates; rate_equations_jit.py:92-136), cooperatively on the
+// group's G lanes: lane t owns column k = c*G + t (slot c) of
+//   M'[r][k] = sum_e R[k,e] BR[e,r] - delta_rk Rk[k],  row n_g - 1 := 1
+// (group_build), eliminates with partial pivoting and back-substitutes
+// M' x = e_last (group_factor).  On return A holds the factors (L
+// below the diagonal, U on and above it), invU the reciprocal pivots of the
+// owned columns (0 below 1e-30), prows the row interchanges (also in
+// `swapped` whether any was taken) and xs the unnormalised populations.
+// Pivot search: partial pivoting takes row col unless some row below holds a
+// strictly larger |A[r][col]|, so the owner of column col first only tests
+// for such a row; the search and interchange run when some group of the warp
+// found one (a warp-uniform branch).  The rows chosen are those of the plain
+// search in every case.  KEEP_L = false (force without adjoint): the L factors
+// are not kept, and every lane updates all of its column slots below the
+// pivot row, including columns at or left of the pivot, whose entries there
+// are never read again (back substitution reads U only); the elimination then
+// runs without per-lane predicates.
+template <int NGMAX, int NEMAX, int G, bool EXACT, bool KEEP_L = true>
+__device__ __forceinline__ void group_factor(const ForceParams &P, int t, int gbase,
+                                             double (&A)[GroupShape<NGMAX, NEMAX, G>::CPL][NGMAX],
+                                             double (&invU)[GroupShape<NGMAX, NEMAX, G>::CPL],
+                                             int (&prows)[NGMAX], bool &swapped,
+                                             double (&xs)[GroupShape<NGMAX, NEMAX, G>::CPL], int &stat)
+{
+    constexpr int CPL = GroupShape<NGMAX, NEMAX, G>::CPL;
+    constexpr unsigned FULL = 0xffffffffu;
+    const int n_g = EXACT ? NGMAX : P.n_g;
+    // right-hand side e_last, distributed like the columns: bs[c] = b[c*G + t]
+    double bs[CPL];
+#pragma unroll
+    for (int c = 0; c < CPL; c++) bs[c] = (c * G + t == n_g - 1) ? 1.0 : 0.0;
+
+    // ---------------- LU with partial pivoting ----------------
+#pragma unroll
+    for (int c = 0; c < CPL; c++) invU[c] = 0.0;
+    swapped = false;
+    static_for<0, NGMAX>([&](auto colc) {
+        constexpr int col = decltype(colc)::value;
+        constexpr int own = col % G, lc = col / G;
+        prows[col] = col;
+        if (EXACT || col < n_g) {
+            bool larger = false;  // some row below holds a strictly larger |A[r][col]|
+            if (t == own) {
+                const double ad = fabs(A[lc][col]);
+#pragma unroll
+                for (int r = col + 1; r < NGMAX; r++)
+                    if (EXACT || r < n_g) larger = larger || (fabs(A[lc][r]) > ad);
+            }
+            if (__any_sync(FULL, larger)) {
+                int prow = col;
+                if (t == own) {
+                    double mx = fabs(A[lc][col]);
+#pragma unroll
+                    for (int r = col + 1; r < NGMAX; r++) {
+                        const double av = fabs(A[lc][r]);
+                        if ((EXACT || r < n_g) && av > mx) { mx = av; prow = r; }
+                    }
+                }
+                prow = __shfl_sync(FULL, prow, gbase + own);
+                prows[col] = prow;
+                if (prow != col) swapped = true;
+                if (prow != col) {
+                    // rows col <-> prow through a local copy indexed at run time
+                    // (rare: predicated register moves for every candidate row
+                    // raised the register pressure of the whole elimination)
+                    double Al[CPL][NGMAX];
+#pragma unroll
+                    for (int c = 0; c < CPL; c++)
+#pragma unroll
+                        for (int r = col; r < NGMAX; r++) Al[c][r] = A[c][r];
+#pragma unroll
+                    for (int c = 0; c < CPL; c++) {
+                        const double tmp = Al[c][col]; Al[c][col] = Al[c][prow]; Al[c][prow] = tmp;
+                    }
+#pragma unroll
+                    for (int c = 0; c < CPL; c++)
+#pragma unroll
+                        for (int r = col; r < NGMAX; r++) A[c][r] = Al[c][r];
+                }
+                // b[col] <-> b[prow]: b[col] sits on lane own (slot lc), b[prow] on lane prow % G
+                double bp = 0.0;
+#pragma unroll
+                for (int c = 0; c < CPL; c++)
+                    if (c * G + t == prow) bp = bs[c];
+                bp = __shfl_sync(FULL, bp, gbase + prow % G);
+                const double bc = __shfl_sync(FULL, bs[lc], gbase + own);
+                if (prow != col) {
+                    if (t == own) bs[lc] = bp;
+#pragma unroll
+                    for (int c = 0; c < CPL; c++)
+                        if (c * G + t == prow) bs[c] = bc;
+                }
+            }
+            double inv_e = 0.0;
+            if (t == own) {
+                const double pv = A[lc][col];
+                const double ap = fabs(pv);
+                const double y = mm_rcp(ap >= 1e-30 ? pv : 1.0);
+                // elimination is skipped below 1e-30, back-substitution needs > 1e-30
+                inv_e = (ap < 1e-30) ? 0.0 : y;
+                invU[lc] = (ap > 1e-30) ? y : 0.0;
+                if (ap < 1e-30) stat |= MM_ST_PIVOT;
+            }
+            const double bcol = __shfl_sync(FULL, bs[lc], gbase + own);  // b[col], final from here on
+#pragma unroll
+            for (int r = col + 1; r < NGMAX; r++) {
+                if (EXACT || r < n_g) {
+                    double f;
+                    if constexpr (KEEP_L) {
+                        f = 0.0;
+                        if (t == own) { f = A[lc][r] * inv_e; A[lc][r] = f; }  // keep the L factor
+                    } else {
+                        f = A[lc][r] * inv_e;  // inv_e = 0 off the owner; only the owner's f is used
+                    }
+                    f = __shfl_sync(FULL, f, gbase + own);
+                    static_for<0, CPL>([&](auto cc) {
+                        constexpr int c = decltype(cc)::value;
+                        if constexpr (c * G > col) {
+                            A[c][r] = fma(-f, A[c][col], A[c][r]);
+                        } else if constexpr (c * G + G - 1 > col) {
+                            if constexpr (KEEP_L) {
+                                if (c * G + t > col) A[c][r] = fma(-f, A[c][col], A[c][r]);
+                            } else {
+                                A[c][r] = fma(-f, A[c][col], A[c][r]);
+                            }
+                        }
+                    });
+                    if (r % G == t) bs[r / G] = fma(-f, bcol, bs[r / G]);
+                }
+            }
+        }
+    });
+
+    // ---------------- back substitution ----------------
+#pragma unroll
+    for (int c = 0; c < CPL; c++) xs[c] = 0.0;
+    static_for<0, NGMAX>([&](auto iic) {
+        constexpr int i = NGMAX - 1 - decltype(iic)::value;
+        constexpr int own = i % G, li = i / G;
+        if (EXACT || i < n_g) {
+            double part = 0.0;
+            static_for<0, CPL>([&](auto cc) {
+                constexpr int c = decltype(cc)::value;
+                if constexpr (c * G > i) {
+                    part = fma(A[c][i], xs[c], part);
+                } else if constexpr (c * G + G - 1 > i) {
+                    if (c * G + t > i) part = fma(A[c][i], xs[c], part);
+                }
+            });
+            part = mm_group_sum(part, G);
+            if (t == own) xs[li] = (bs[li] - part) * invU[li];
+        }
+    });
+}
+
+// Clamp, normalise (uniform populations when all clamp, if asked), and the
+// point's force and scattering rate, identical in every lane of the group.
+template <int NGMAX, int NEMAX, int G, bool EXACT>
+__device__ __forceinline__ PointOut group_finish(const ForceParams &P, int t,
+                                                 double (&xs)[GroupShape<NGMAX, NEMAX, G>::CPL],
+                                                 const double (&Fk)[GroupShape<NGMAX, NEMAX, G>::CPL],
+                                                 const double (&Rk)[GroupShape<NGMAX, NEMAX, G>::CPL],
+                                                 int &stat)
+{
+    constexpr int CPL = GroupShape<NGMAX, NEMAX, G>::CPL;
+    const int n_g = EXACT ? NGMAX : P.n_g;
+    double tot = 0.0;
+#pragma unroll
+    for (int c = 0; c < CPL; c++) {
+        const int j = c * G + t;
+        if (EXACT ? (j < NGMAX) : (j < n_g)) { if (xs[c] < 0.0) xs[c] = 0.0; }
+        else xs[c] = 0.0;
+        tot += xs[c];
+    }
+    tot = mm_group_sum(tot, G);
+    if (tot > 0.0) {
+        const double it = mm_rcp(tot);
+#pragma unroll
+        for (int c = 0; c < CPL; c++) xs[c] *= it;
+    } else {
+        stat |= MM_ST_ZERO_POP;
+        if (P.uniform_fb) {
+            const double u = 1.0 / (double)n_g;
+#pragma unroll
+            for (int c = 0; c < CPL; c++) xs[c] = (c * G + t < n_g) ? u : 0.0;
+        }
+    }
+    double F = 0.0, Rs = 0.0;
+#pragma unroll
+    for (int c = 0; c < CPL; c++) {
+        if (EXACT ? (c * G + t < NGMAX) : (c * G + t < n_g)) {
+            F = fma(xs[c], Fk[c], F);
+            Rs = fma(xs[c], Rk[c], Rs);
+        }
+    }
+    PointOut out;
+    out.F = mm_group_sum(F, G);
+    out.R = mm_group_sum(Rs, G);
+    out.gB = 0.0;
+    out.status = 0;
+    return out;
+}
+
+// Multipliers of the adjoint: lambda solving M'^T lambda = F_g (the ground
+// states' force terms) with the factors of group_factor<KEEP_L = true>,
+// P M' = L U:  U^T w = F, L^T u = w, lambda = P^T u (replicated in every lane
+// of the group), and nu[e] = sum_{g < n_g - 1} lambda_g BR[e,g].
+template <int NGMAX, int NEMAX, int G, bool EXACT>
+__device__ __forceinline__ void group_lambda(const ForceParams &P, const double *BR, int se, int sr, int t,
+                                             int gbase,
+                                             const double (&A)[GroupShape<NGMAX, NEMAX, G>::CPL][NGMAX],
+                                             const double (&invU)[GroupShape<NGMAX, NEMAX, G>::CPL],
+                                             const int (&prows)[NGMAX], bool swapped,
+                                             const double (&Fk)[GroupShape<NGMAX, NEMAX, G>::CPL],
+                                             double (&wv)[NGMAX], double (&nu)[NEMAX])
+{
+    constexpr unsigned FULL = 0xffffffffu;
+    const int n_g = EXACT ? NGMAX : P.n_g;
+    const int n_e = EXACT ? NEMAX : P.n_e;
+    static_for<0, NGMAX>([&](auto ic) {
+        constexpr int i = decltype(ic)::value;
+        constexpr int own = i % G, li = i / G;
+        double wi = 0.0;
+        if (EXACT || i < n_g) {
+            if (t == own) {
+                double sacc = Fk[li];
+#pragma unroll
+                for (int j = 0; j < i; j++) sacc = fma(-A[li][j], wv[j], sacc);  // U[j][i]
+                wi = sacc * invU[li];
+            }
+            wi = __shfl_sync(FULL, wi, gbase + own);
+        }
+        wv[i] = wi;
+    });
+    static_for<0, NGMAX>([&](auto iic) {
+        constexpr int i = NGMAX - 1 - decltype(iic)::value;
+        constexpr int own = i % G, li = i / G;
+        if (EXACT || i < n_g) {
+            double ui = 0.0;
+            if (t == own) {
+                double sacc = wv[i];
+#pragma unroll
+                for (int j = i + 1; j < NGMAX; j++)
+                    if (EXACT || j < n_g) sacc = fma(-A[li][j], wv[j], sacc);  // L[j][i]
+                ui = sacc;
+            }
+            wv[i] = __shfl_sync(FULL, ui, gbase + own);
+        }
+    });
+    if (__any_sync(FULL, swapped)) {
+#pragma unroll
+        for (int col = NGMAX - 1; col >= 0; col--) {
+#pragma unroll
+            for (int r = col + 1; r < NGMAX; r++)
+                if (r == prows[col]) { const double tmp = wv[col]; wv[col] = wv[r]; wv[r] = tmp; }
+        }
+    }
+#pragma unroll
+    for (int e = 0; e < NEMAX; e++) {
+        double a = 0.0;
+#pragma unroll
+        for (int g = 0; g < NGMAX; g++)
+            if (g < n_g - 1 && e < n_e) a = fma(wv[g], BR[e * se + g * sr], a);
+        nu[e] = a;
+    }
+}
+
 // Solve one point.  xs[c] receives p[c*G + t] for the owned columns.
 // fd / Ese: this group's scratch (n_b + n_e doubles) in shared memory
 // (FP64 form only).  EXACT: the molecule has exactly NGMAX ground and NEMAX
 // excited states (size predicates vanish at compile time).
-template <int NGMAX, int NEMAX, int G, bool EXACT, bool ADJ = false>
+template <int NGMAX, int NEMAX, int G, bool EXACT>
 __device__ __forceinline__ PointOut solve_point(const ForceParams &P, const SetView &S, double *fd,
                                                 double *Ese, int t, int gbase, double v, double z,
                                                 double Bgrad,
-                                                double (&xs)[GroupShape<NGMAX, NEMAX, G>::CPL],
-                                                double *gacc = nullptr)
+                                                double (&xs)[GroupShape<NGMAX, NEMAX, G>::CPL])
 {
     constexpr int CPL = GroupShape<NGMAX, NEMAX, G>::CPL;
-    constexpr unsigned FULL = 0xffffffffu;
     const int n_g = EXACT ? NGMAX : P.n_g;
     const int n_e = EXACT ? NEMAX : P.n_e;
     const double gh = P.Gamma / 2.0;
@@ -245,7 +551,7 @@ __device__ __forceinline__ PointOut solve_point(const ForceParams &P, const SetV
 
     // ---------------- rates of the owned ground states ----------------
     double R[CPL][NEMAX];
-    double Fk[CPL], Rk[CPL], satk[CPL];
+    double Fk[CPL], Rk[CPL];
     const double B_gauss = __dmul_rn(__dmul_rn(Bgrad, z), 1e4);
     __syncwarp();
     // laser frequency seen by the moving molecule, per beam (exact order)
@@ -289,7 +595,6 @@ __device__ __forceinline__ PointOut solve_point(const ForceParams &P, const SetV
         }
         // saturation correction 1/(1 + s_total[g]) (rate_equations_jit.py:85-90)
         const double sat = mm_rcp(1.0 + s);
-        satk[c] = sat;
         double rs = 0.0;
 #pragma unroll
         for (int e = 0; e < NEMAX; e++) {
@@ -300,261 +605,12 @@ __device__ __forceinline__ PointOut solve_point(const ForceParams &P, const SetV
         Fk[c] = f * sat;
     }
 
-    // ---------------- columns of M' (FP64), replicated right-hand side ----------------
-    double A[CPL][NGMAX];
-    double b[NGMAX];
-#pragma unroll
-    for (int r = 0; r < NGMAX; r++) {
-        b[r] = (r == n_g - 1) ? 1.0 : 0.0;
-        double br[NEMAX];
-#pragma unroll
-        for (int e = 0; e < NEMAX; e++) br[e] = (r < n_g && e < n_e) ? S.BR[e * n_g + r] : 0.0;
-#pragma unroll
-        for (int c = 0; c < CPL; c++) {
-            const int j = c * G + t;
-            double a;
-            if (EXACT || j < n_g) {
-                a = (r == j) ? -Rk[c] : 0.0;
-#pragma unroll
-                for (int e = 0; e < NEMAX; e++) a = fma(R[c][e], br[e], a);
-                if (r == n_g - 1) a = 1.0;           // normalisation row
-                if (!EXACT && r >= n_g) a = 0.0;
-            } else {
-                a = (r == j) ? 1.0 : 0.0;            // identity padding beyond n_g
-            }
-            A[c][r] = a;
-        }
-    }
-
-    // ---------------- LU with partial pivoting ----------------
-    double invU[CPL];
-#pragma unroll
-    for (int c = 0; c < CPL; c++) invU[c] = 0.0;
+    double A[CPL][NGMAX], invU[CPL];
     int prows[NGMAX];
-    bool swapped = false;
-    static_for<0, NGMAX>([&](auto colc) {
-        constexpr int col = decltype(colc)::value;
-        constexpr int own = col % G, lc = col / G;
-        prows[col] = col;
-        if (EXACT || col < n_g) {
-            int prow = col;
-            if (t == own) {
-                double mx = fabs(A[lc][col]);
-#pragma unroll
-                for (int r = col + 1; r < NGMAX; r++) {
-                    const double av = fabs(A[lc][r]);
-                    if ((EXACT || r < n_g) && av > mx) { mx = av; prow = r; }
-                }
-            }
-            prow = __shfl_sync(FULL, prow, gbase + own);
-            prows[col] = prow;
-            if (__any_sync(FULL, prow != col)) {
-                swapped = true;
-#pragma unroll
-                for (int r = col + 1; r < NGMAX; r++) {
-                    if (r == prow) {
-#pragma unroll
-                        for (int c = 0; c < CPL; c++) {
-                            const double tmp = A[c][col]; A[c][col] = A[c][r]; A[c][r] = tmp;
-                        }
-                        const double tb = b[col]; b[col] = b[r]; b[r] = tb;
-                    }
-                }
-            }
-            double inv_e = 0.0;
-            if (t == own) {
-                const double pv = A[lc][col];
-                const double ap = fabs(pv);
-                const double y = mm_rcp(ap >= 1e-30 ? pv : 1.0);
-                // elimination is skipped below 1e-30, back-substitution needs > 1e-30
-                inv_e = (ap < 1e-30) ? 0.0 : y;
-                invU[lc] = (ap > 1e-30) ? y : 0.0;
-                if (ap < 1e-30) stat |= MM_ST_PIVOT;
-            }
-#pragma unroll
-            for (int r = col + 1; r < NGMAX; r++) {
-                if (EXACT || r < n_g) {
-                    double f = 0.0;
-                    if (t == own) { f = A[lc][r] * inv_e; A[lc][r] = f; }  // keep the L factor
-                    f = __shfl_sync(FULL, f, gbase + own);
-                    static_for<0, CPL>([&](auto cc) {
-                        constexpr int c = decltype(cc)::value;
-                        if constexpr (c * G > col) {
-                            A[c][r] = fma(-f, A[c][col], A[c][r]);
-                        } else if constexpr (c * G + G - 1 > col) {
-                            if (c * G + t > col) A[c][r] = fma(-f, A[c][col], A[c][r]);
-                        }
-                    });
-                    b[r] = fma(-f, b[col], b[r]);
-                }
-            }
-        }
-    });
-
-    // ---------------- back substitution ----------------
-#pragma unroll
-    for (int c = 0; c < CPL; c++) xs[c] = 0.0;
-    static_for<0, NGMAX>([&](auto iic) {
-        constexpr int i = NGMAX - 1 - decltype(iic)::value;
-        constexpr int own = i % G, li = i / G;
-        if (EXACT || i < n_g) {
-            double part = 0.0;
-            static_for<0, CPL>([&](auto cc) {
-                constexpr int c = decltype(cc)::value;
-                if constexpr (c * G > i) {
-                    part = fma(A[c][i], xs[c], part);
-                } else if constexpr (c * G + G - 1 > i) {
-                    if (c * G + t > i) part = fma(A[c][i], xs[c], part);
-                }
-            });
-            part = mm_group_sum(part, G);
-            if (t == own) xs[li] = (b[i] - part) * invU[li];
-        }
-    });
-
-    // ---------------- clamp, normalise, force ----------------
-    double tot = 0.0;
-#pragma unroll
-    for (int c = 0; c < CPL; c++) {
-        const int j = c * G + t;
-        if (EXACT ? (j < NGMAX) : (j < n_g)) { if (xs[c] < 0.0) xs[c] = 0.0; }
-        else xs[c] = 0.0;
-        tot += xs[c];
-    }
-    tot = mm_group_sum(tot, G);
-    if (tot > 0.0) {
-        const double it = mm_rcp(tot);
-#pragma unroll
-        for (int c = 0; c < CPL; c++) xs[c] *= it;
-    } else {
-        stat |= MM_ST_ZERO_POP;
-        if (P.uniform_fb) {
-            const double u = 1.0 / (double)n_g;
-#pragma unroll
-            for (int c = 0; c < CPL; c++) xs[c] = (c * G + t < n_g) ? u : 0.0;
-        }
-    }
-    double F = 0.0, Rs = 0.0;
-#pragma unroll
-    for (int c = 0; c < CPL; c++) {
-        if (EXACT ? (c * G + t < NGMAX) : (c * G + t < n_g)) {
-            F = fma(xs[c], Fk[c], F);
-            Rs = fma(xs[c], Rk[c], Rs);
-        }
-    }
-    PointOut out;
-    out.F = mm_group_sum(F, G);
-    out.R = mm_group_sum(Rs, G);
-    out.gB = 0.0;
-    if constexpr (ADJ) {
-        // ---------- adjoint: dF/dtheta = sum_{b,g,e} (p_g hk_b - mu[g,e]) d rate_bge / dtheta ----------
-        // with lambda solving M'^T lambda = dF/dp = F_g and
-        // mu[g,e] = p_g (sum_{g'<n-1} lambda_g' BR[e,g'] - lambda_g [g<n-1]) (implicit differentiation
-        // of M' p = e_last on the fixed active set; the last row of M' is constant).
-        // Transposed solve with the stored factors, P M' = L U:  U^T w = F, L^T u = w, lambda = P^T u.
-        double wv[NGMAX];
-        static_for<0, NGMAX>([&](auto ic) {
-            constexpr int i = decltype(ic)::value;
-            constexpr int own = i % G, li = i / G;
-            double wi = 0.0;
-            if (EXACT || i < n_g) {
-                if (t == own) {
-                    double sacc = Fk[li];
-#pragma unroll
-                    for (int j = 0; j < i; j++) sacc = fma(-A[li][j], wv[j], sacc);  // U[j][i]
-                    wi = sacc * invU[li];
-                }
-                wi = __shfl_sync(FULL, wi, gbase + own);
-            }
-            wv[i] = wi;
-        });
-        static_for<0, NGMAX>([&](auto iic) {
-            constexpr int i = NGMAX - 1 - decltype(iic)::value;
-            constexpr int own = i % G, li = i / G;
-            if (EXACT || i < n_g) {
-                double ui = 0.0;
-                if (t == own) {
-                    double sacc = wv[i];
-#pragma unroll
-                    for (int j = i + 1; j < NGMAX; j++)
-                        if (EXACT || j < n_g) sacc = fma(-A[li][j], wv[j], sacc);  // L[j][i]
-                    ui = sacc;
-                }
-                wv[i] = __shfl_sync(FULL, ui, gbase + own);
-            }
-        });
-        if (__any_sync(FULL, swapped)) {
-#pragma unroll
-            for (int col = NGMAX - 1; col >= 0; col--) {
-#pragma unroll
-                for (int r = col + 1; r < NGMAX; r++)
-                    if (r == prows[col]) { const double tmp = wv[col]; wv[col] = wv[r]; wv[r] = tmp; }
-            }
-        }
-        double nu[NEMAX];
-#pragma unroll
-        for (int e = 0; e < NEMAX; e++) {
-            double a = 0.0;
-#pragma unroll
-            for (int g = 0; g < NGMAX; g++)
-                if (g < n_g - 1 && e < n_e) a = fma(wv[g], S.BR[e * n_g + g], a);
-            nu[e] = a;
-        }
-        // per-beam accumulators (this group's shared scratch): dF/dfreq_b, dF/ds0_b
-        for (int i = t; i < 2 * P.n_b; i += G) gacc[i] = 0.0;
-        __syncwarp();
-        const double geff = P.geff;
-        double gB = 0.0;
-#pragma unroll
-        for (int c = 0; c < CPL; c++) {
-            const int k = c * G + t;
-            const bool own = EXACT ? (k < NGMAX) : (k < n_g);
-            const int kk = own ? k : 0;
-            const int cntk = own ? S.cnt[kk] : 0;
-            const int o = S.off[kk];
-            const int mc = S.maxcnt[c];
-            double lamk = 0.0;
-#pragma unroll
-            for (int g = c * G; g < c * G + G && g < NGMAX; g++)
-                if (g == k) lamk = wv[g];
-            const double pk = xs[c], sat = satk[c];
-            double mu[NEMAX];
-#pragma unroll
-            for (int e = 0; e < NEMAX; e++) mu[e] = pk * (nu[e] - ((k < n_g - 1) ? lamk : 0.0));
-            const double Esg = fma(B_gauss, S.czd[kk], S.E[kk]);
-            double T = 0.0;
-            for (int pass = 0; pass < 2; pass++) {
-                const double C = T * sat;
-                for (int i = 0; i < mc; i++) {
-                    if (i < cntk) {
-                        const Trip64 tr = S.t64[o + i];
-                        const int b = tr.be & 0xff, e = tr.be >> 8;
-                        const double om = __dsub_rn(Ese[e], Esg);
-                        const double de = __dmul_rn(__dsub_rn(fd[b], om), MM_TWO_PI);
-                        const double L = gh2 * mm_rcp(fma(de, de, gh2));
-                        const double rate = tr.c1g * L * sat;
-                        double mue = 0.0;
-#pragma unroll
-                        for (int ee = 0; ee < NEMAX; ee++)
-                            if (ee == e) mue = mu[ee];
-                        const double w = pk * tr.hk - mue;
-                        if (pass == 0) {
-                            T = fma(w, rate, T);
-                        } else {
-                            const double Q = w * rate - C * tr.c2 * L;
-                            const double dLL = -2.0 * de * L / gh2;  // (dL/d delta) / L
-                            atomicAdd(&gacc[b], Q * dLL * MM_TWO_PI);
-                            atomicAdd(&gacc[P.n_b + b], S.d2t[o + i] * L * (w * gh * geff * sat - C));
-                            const double ddB = -z * 1e4 * (S.zd[n_g + e] - S.zd[kk]) * P.Gamma;
-                            gB = fma(Q * dLL, ddB, gB);
-                        }
-                    }
-                }
-            }
-        }
-        out.gB = mm_group_sum(gB, G);
-        __syncwarp();
-    }
+    bool swapped;
+    group_build<NGMAX, NEMAX, G, EXACT>(P, S.BR, n_g, 1, t, R, Rk, A);
+    group_factor<NGMAX, NEMAX, G, EXACT>(P, t, gbase, A, invU, prows, swapped, xs, stat);
+    PointOut out = group_finish<NGMAX, NEMAX, G, EXACT>(P, t, xs, Fk, Rk, stat);
     if (!isfinite(out.F)) stat |= MM_ST_NONFINITE;
     out.status = mm_group_or(stat, G);
     return out;

@@ -123,7 +123,10 @@ def test_adjoint_forward_equals_force_batch(mol, gpu):
     bs = BeamSets(sel(g["kdir"]), sel(g["freq"]), sel(g["pol"]), sel(g["s0"]), sel(g["B"]))
     F, G = force_adjoint(pack_for(mol), bs, g["v"], g["z"], points_per_set=npts)
     F2 = force_batch(pack_for(mol), bs, g["v"], g["z"], points_per_set=npts)["F"]
-    assert torch.equal(F, F2)
+    # same rates, matrix and elimination; the force maps split a point over 2
+    # lanes and the adjoint over 4, so the back-substitution and normalisation
+    # sums associate differently: equal to rounding
+    assert float((F - F2).abs().max()) <= 1e-14 * float(F2.abs().max())
     assert G.shape == (ns * npts, 17)
 
 
