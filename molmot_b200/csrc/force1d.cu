@@ -191,16 +191,20 @@ force_plain_kernel(ForceParams P)
 //     force_plain_kernel, plus each ground state's saturation factor;
 //  2. groups of G lanes: the elimination keeping L (group_factor), the
 //     populations and force (group_finish), and the multipliers lambda and nu
-//     of the transposed solve (group_lambda); p_g and lambda_g replace the
-//     first two rate rows of the point's column, nu goes to its own table;
-//  3. one thread per point: the two passes over each ground state's triples
+//     of the transposed solve (group_lambda); also, per ground state,
+//     T_g = sum over its triples of (p_g hk_b - mu[g,e]) rate_bge, which
+//     equals p_g F_g - sum_e mu[g,e] R[g,e] from the table's own sums.  p_g,
+//     lambda_g and T_g replace rate rows 0, 1 and the force row of the
+//     point's column, nu goes to its own table;
+//  3. one thread per point: one pass over each ground state's triples
 //     (dF/dtheta = sum (p_g hk_b - mu[g,e]) d rate_bge / dtheta, with
-//     mu[g,e] = p_g (nu_e - lambda_g [g < n_g - 1])) into the thread's own
-//     accumulators (no atomics; a fixed summation order).
+//     mu[g,e] = p_g (nu_e - lambda_g [g < n_g - 1]); the saturation term
+//     through T_g) into the thread's own accumulators (no atomics; a fixed
+//     summation order).
 // grad row layout per point: [dF/dfreq_0 .. dF/dfreq_{nb-1}, dF/ds0_0 ..
 // dF/ds0_{nb-1}, dF/dB'].
 template <int NGMAX, int NEMAX, bool EXACT, int PAD, int TH, int G>
-__global__ void __launch_bounds__(TH, 3)
+__global__ void __launch_bounds__(TH, (TH <= 64 ? 3 : 2))
 force_plain_adjoint_kernel(ForceParams P, double *grad)
 {
     using GS = GroupShape<NGMAX, NEMAX, G>;
@@ -310,19 +314,37 @@ force_plain_adjoint_kernel(ForceParams P, double *grad)
                                                      wv, nu);
                 if (!isfinite(o.F)) stat |= MM_ST_NONFINITE;
                 o.status = mm_group_or(stat, G);
+                // T_k = sum over k's triples of (p_k hk_b - mu[k,e]) rate_bke
+                //     = p_k F_k - sum_e mu[k,e] R[k,e]   (F_k, R[k,e] saturated)
+                double Tk[CPL], lk[CPL];
+#pragma unroll
+                for (int c = 0; c < CPL; c++) {
+                    const int k = c * G + t;
+                    const bool own = EXACT ? (k < NGMAX) : (k < n_g);
+                    const double *row = rtab + (size_t)(own ? k : 0) * RBS + p;
+                    double lam = 0.0;
+#pragma unroll
+                    for (int g = 0; g < NGMAX; g++)
+                        if (g == k) lam = wv[g];
+                    lk[c] = lam;
+                    double T = xs[c] * Fk[c];
+#pragma unroll
+                    for (int e = 0; e < NEMAX; e++) {
+                        const double mue = xs[c] * (nu[e] - ((k < n_g - 1) ? lam : 0.0));
+                        T = fma(-mue, own ? row[e * TH] : 0.0, T);
+                    }
+                    Tk[c] = T;
+                }
                 __syncwarp();
-                // p_g and lambda_g over the first two rate rows of the point (read above)
+                // p_k, lambda_k and T_k over rows 0, 1 and NEMAX (F) of the point's column
 #pragma unroll
                 for (int c = 0; c < CPL; c++) {
                     const int k = c * G + t;
                     if (EXACT ? (k < NGMAX) : (k < n_g)) {
                         double *row = rtab + (size_t)k * RBS + p;
-                        double lam = 0.0;
-#pragma unroll
-                        for (int g = 0; g < NGMAX; g++)
-                            if (g == k) lam = wv[g];
                         row[0] = xs[c];
-                        row[TH] = lam;
+                        row[TH] = lk[c];
+                        row[NEMAX * TH] = Tk[c];
                     }
                 }
                 if (t == 0) {
@@ -345,36 +367,29 @@ force_plain_adjoint_kernel(ForceParams P, double *grad)
 #pragma unroll
                 for (int e = 0; e < NEMAX; e++) nue[e] = nut[e * TH + tid];
                 double gB = 0.0;
+                const double igh2 = 1.0 / gh2;
                 for (int g = 0; g < n_g; g++) {
                     const double *row = rtab + (size_t)g * RBS + tid;
                     const double pk = row[0], lamk = row[TH], sat = row[(NEMAX + 1) * TH];
+                    const double Cs = row[NEMAX * TH] * sat;  // T_g sat (saturation term)
                     const double Esg = fma(C.B, S.czd[g], S.E[g]);
-                    double T = 0.0;
-#pragma unroll 1
-                    for (int pass = 0; pass < 2; pass++) {
-                        const double Cs = T * sat;
 #pragma unroll
-                        for (int e = 0; e < NEMAX; e++) {
-                            const double mue = pk * (nue[e] - ((g < n_g - 1) ? lamk : 0.0));
-                            const double ddB = (e < n_e) ? -z * 1e4 * (P.zd[n_g + e] - P.zd[g]) * P.Gamma : 0.0;
-                            const int i1 = S.offs[g * NEMAX + e + 1];
-                            for (int i = S.offs[g * NEMAX + e]; i < i1; i++) {
-                                const TripD tr = ((const TripD *)S.trip)[i];
-                                const double om = __dsub_rn(C.Ese[e], Esg);
-                                const double de = __dmul_rn(__dsub_rn(fds[tr.b * TH + tid], om), MM_TWO_PI);
-                                const double L = gh2 * mm_rcp(fma(de, de, gh2));
-                                const double rate = tr.c1 * L * sat;
-                                const double w = pk * tr.hk - mue;
-                                if (pass == 0) {
-                                    T = fma(w, rate, T);
-                                } else {
-                                    const double Q = w * rate - Cs * tr.c2 * L;
-                                    const double dLL = -2.0 * de * L / gh2;  // (dL/d delta) / L
-                                    gas[tr.b * TH + tid] += Q * dLL * MM_TWO_PI;
-                                    gas[(nb + tr.b) * TH + tid] += S.d2t[i] * L * (w * gh * geff * sat - Cs);
-                                    gB = fma(Q * dLL, ddB, gB);
-                                }
-                            }
+                    for (int e = 0; e < NEMAX; e++) {
+                        const double mue = pk * (nue[e] - ((g < n_g - 1) ? lamk : 0.0));
+                        const double ddB = (e < n_e) ? -z * 1e4 * (P.zd[n_g + e] - P.zd[g]) * P.Gamma : 0.0;
+                        const int i1 = S.offs[g * NEMAX + e + 1];
+                        for (int i = S.offs[g * NEMAX + e]; i < i1; i++) {
+                            const TripD tr = ((const TripD *)S.trip)[i];
+                            const double om = __dsub_rn(C.Ese[e], Esg);
+                            const double de = __dmul_rn(__dsub_rn(fds[tr.b * TH + tid], om), MM_TWO_PI);
+                            const double L = gh2 * mm_rcp1(fma(de, de, gh2));  // feeds the gradient only
+                            const double rate = tr.c1 * L * sat;
+                            const double w = pk * tr.hk - mue;
+                            const double Q = w * rate - Cs * tr.c2 * L;
+                            const double dLL = -2.0 * de * L * igh2;  // (dL/d delta) / L
+                            gas[tr.b * TH + tid] += Q * dLL * MM_TWO_PI;
+                            gas[(nb + tr.b) * TH + tid] += S.d2t[i] * L * (w * gh * geff * sat - Cs);
+                            gB = fma(Q * dLL, ddB, gB);
                         }
                     }
                 }
@@ -995,7 +1010,11 @@ int launch_traj_reduced(const ForceParams &P, const TrajParams &T, cudaStream_t 
 }
 
 
-constexpr int kPlainAdjThreads = 64;
+// rounds of 96 points: 2 CTAs per SM (the tables take 93 KB for SrOH); on
+// 1024 sets x 66 stencil points this took 0.257 ms against 0.287 ms with
+// rounds of 64 (3 CTAs per SM, but a second round for 2 points of every
+// set) and 0.432 ms with rounds of 128 (one CTA per SM)
+constexpr int kPlainAdjThreads = 96;
 constexpr int kPlainAdjG = 4;
 
 template <class C, int PAD>

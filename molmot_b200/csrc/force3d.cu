@@ -679,21 +679,25 @@ traj3d_kernel(Force3Params P, Traj3Params T)
     long long na = T.step0 + T.n_steps;
     long long nev = 0;
     const long long row = ipc * T.n_steps * 3;
-    if (T.step0 == 0) {
-        if (valid && T.r_traj && t == 0)
-            for (int c = 0; c < 3; c++) { T.r_traj[row + c] = r[c]; T.v_traj[row + c] = vh[c]; }
-        const Out3 o = force3d_point(P, S, S.grp[group], t, gbase, r, vh, Bg, pl);
-        for (int c = 0; c < 3; c++) vh[c] = vh[c] + 0.5 * dt * o.F[c] / m;
-    }
-    const long long j0 = (T.step0 == 0) ? 1 : T.step0;
+    if (T.step0 == 0 && valid && T.r_traj && t == 0)
+        for (int c = 0; c < 3; c++) { T.r_traj[row + c] = r[c]; T.v_traj[row + c] = vh[c]; }
+    // iteration j = 0 (a run from step 0) is the first half kick at (r0, v0);
+    // it shares the loop's single inlined force evaluation (two call sites
+    // doubled the kernel's code and its instruction-cache misses)
+    const long long j0 = (T.step0 == 0) ? 0 : T.step0;
     const long long j1 = T.step0 + T.n_steps;
     for (long long j = j0; j < j1; j++) {
         if (__all_sync(0xffffffffu, done)) break;
+        const bool kick0 = j == 0;  // the same on every lane
         double rn[3];
-        for (int c = 0; c < 3; c++) rn[c] = __dadd_rn(r[c], __dmul_rn(dt, vh[c]));  // r + dt v_half
+        for (int c = 0; c < 3; c++) rn[c] = kick0 ? r[c] : __dadd_rn(r[c], __dmul_rn(dt, vh[c]));  // r + dt v_half
         const double rr = sqrt(rn[0] * rn[0] + rn[1] * rn[1] + rn[2] * rn[2]);
-        const bool esc = !done && rr > T.r_escape;
+        const bool esc = !done && !kick0 && rr > T.r_escape;
         const Out3 o = force3d_point(P, S, S.grp[group], t, gbase, rn, vh, Bg, pl);
+        if (kick0) {
+            for (int c = 0; c < 3; c++) vh[c] = vh[c] + 0.5 * dt * o.F[c] / m;
+            continue;
+        }
         if (!done) {
             for (int c = 0; c < 3; c++) r[c] = rn[c];
             const long long out_j = j - T.step0;
@@ -851,7 +855,9 @@ __device__ void force3d_tangent(const Force3Params &P, const Tg3Params &T, Smem3
             }
         }
         // the forward's population factors, column t
-        for (int i = 0; i < n_g; i++) TW.LU[i][t] = kp.A[i];
+#pragma unroll
+        for (int i = 0; i < NGM; i++)  // compile-time indices keep kp in registers
+            if (i < n_g) TW.LU[i][t] = kp.A[i];
         TW.invd[t] = kp.invd;
     }
     __syncwarp();
@@ -950,6 +956,9 @@ __device__ void force3d_tangent(const Force3Params &P, const Tg3Params &T, Smem3
 #pragma unroll
         for (int e = 0; e < NEM; e++) dRu[e] = 0.0;
         if (lane) {
+            // 1/(Gamma/2)^2 and 1/2pi once: a division in this loop ran for every
+            // (parameter, beam, excited state)
+            const double igh2 = 1.0 / gh2, kInv2Pi = 1.0 / MM_TWO_PI;
             const double Eg = W.Esg[t], dEg = dlam * G / (2 * MM_PI);
             for (int b = 0; b < n_b; b++) {
                 const double fd = __dadd_rn(S.freq[b], W.bm[b][0]);
@@ -963,9 +972,9 @@ __device__ void force3d_tangent(const Force3Params &P, const Tg3Params &T, Smem3
                         const double om = __dsub_rn(W.Ese[e], Eg);
                         const double de = __dmul_rn(__dsub_rn(fd, om), MM_TWO_PI);
                         const double L = gh2 * mm_rcp(fma(de, de, gh2));
-                        const double dEe = dB[2] * S.Ze[e] * G / MM_TWO_PI;
+                        const double dEe = dB[2] * S.Ze[e] * G * kInv2Pi;
                         const double dde = (dfd - (dEe - dEg)) * MM_TWO_PI;
-                        const double dL = -2.0 * de * L * L / gh2 * dde;
+                        const double dL = -2.0 * de * L * L * igh2 * dde;
                         double ws = 0.0, dws = 0.0;
 #pragma unroll
                         for (int q = 0; q < 3; q++) {
@@ -1109,32 +1118,35 @@ traj3d_grad_kernel(Force3Params P, Tg3Params T)
                 }
         }
     };
-    if (T.step0 == 0) {  // first half kick at (r0, v0), as traj3d_kernel
-        set_dirs();
-        const Out3 o = force3d_point(P, S, S.grp[group], t, gbase, r, vh, Bg, pl, &kp);
-        force3d_tangent(P, T, S, S.grp[group], TW, t, r, vh, Bg, kp, stat);
-        for (int c = 0; c < 3; c++) vh[c] = vh[c] + 0.5 * dt * o.F[c] / m;
-        if (t < 3)
-            for (int k = 0; k < np; k++) TW.Tv[t][k] = fma(0.5 * dt / m, TW.dF[k][t], TW.Tv[t][k]);
-        __syncwarp();
-    }
-    const long long j0 = (T.step0 == 0) ? 1 : T.step0;
+    // iteration j = 0 (a run from step 0) is the first half kick at (r0, v0),
+    // as traj3d_kernel; it shares the loop's single inlined force and tangent
+    // evaluation, and runs for every particle, stopped ones included
+    const long long j0 = (T.step0 == 0) ? 0 : T.step0;
     const long long j1 = T.step0 + T.n_steps;
     long long j = j0;
     for (; j < j1; j++) {
-        if (__all_sync(0xffffffffu, done)) break;
+        const bool kick0 = j == 0;  // the same on every lane
+        if (!kick0 && __all_sync(0xffffffffu, done)) break;
         double rn[3];
-        for (int c = 0; c < 3; c++) rn[c] = __dadd_rn(r[c], __dmul_rn(dt, vh[c]));  // r + dt v_half
+        for (int c = 0; c < 3; c++) rn[c] = kick0 ? r[c] : __dadd_rn(r[c], __dmul_rn(dt, vh[c]));  // r + dt v_half
         const double rr = sqrt(rn[0] * rn[0] + rn[1] * rn[1] + rn[2] * rn[2]);
-        const bool esc = !done && rr > T.r_escape;
+        const bool esc = !done && !kick0 && rr > T.r_escape;
         // position tangent first: the force is evaluated at (r_j, v_half)
-        if (!done && t < 3)
+        if (!kick0 && !done && t < 3)
             for (int k = 0; k < np; k++) TW.Tr[t][k] = fma(dt, TW.Tv[t][k], TW.Tr[t][k]);
         __syncwarp();
         set_dirs();
         const Out3 o = force3d_point(P, S, S.grp[group], t, gbase, rn, vh, Bg, pl, &kp);
         int st = 0;
         force3d_tangent(P, T, S, S.grp[group], TW, t, rn, vh, Bg, kp, st);
+        if (kick0) {
+            stat |= st;
+            for (int c = 0; c < 3; c++) vh[c] = vh[c] + 0.5 * dt * o.F[c] / m;
+            if (t < 3)
+                for (int k = 0; k < np; k++) TW.Tv[t][k] = fma(0.5 * dt / m, TW.dF[k][t], TW.Tv[t][k]);
+            __syncwarp();
+            continue;
+        }
         if (!done) {
             stat |= st;
             for (int c = 0; c < 3; c++) r[c] = rn[c];

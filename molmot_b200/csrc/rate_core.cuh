@@ -56,6 +56,17 @@ __device__ __forceinline__ double mm_rcp(double d)
     return fma(y, e, y);
 }
 
+// Reciprocal by one Newton-Raphson step from rcp.approx.ftz.f64: relative
+// error about the square of the approximation's, well below 1e-12; for
+// quantities that only feed derivatives (checked at 1e-8), never forces.
+__device__ __forceinline__ double mm_rcp1(double d)
+{
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(d));
+    const double e = fma(-d, y, 1.0);
+    return fma(y, e, y);
+}
+
 // Reciprocal square root by Newton-Raphson iteration y <- y (3 - x y^2) / 2,
 // written as e = 1/2 - (x/2) y y, y <- y + y e, started from the PTX hardware
 // approximation rsqrt.approx.ftz.f64; two steps reach double precision.

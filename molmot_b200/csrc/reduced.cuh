@@ -764,7 +764,7 @@ __device__ __forceinline__ RedOut reduced_adjoint_point(const ForceParams &P, co
                 if (tr.pad) continue;  // list padding
                 const int b = tr.b;
                 const double de = __dmul_rn(__dsub_rn(fd[b * stride], om), MM_TWO_PI);
-                const double iden = mm_rcp(fma(de, de, gh2));
+                const double iden = mm_rcp1(fma(de, de, gh2));  // feeds the gradient only
                 const double L = gh2 * iden;
                 const double dLd = -2.0 * de * L * iden;  // dL / d delta
                 const double q = fma(alpha + beta * tr.hk, tr.c1, gamma * tr.c2);
