@@ -790,7 +790,7 @@ constexpr int kTgThreads = 128;
 constexpr int kTgSub = 1;             // lanes per axis (each takes every kTgSub-th ground state)
 constexpr int kTgLanes = 4 * kTgSub;  // lanes per particle: x, y, z and an idle slot
 
-template <int NGMAX, int NEMAX, bool EXACT, int PAD>
+template <int NGMAX, int NEMAX, bool EXACT, int PAD, bool KEEP>
 __global__ void __launch_bounds__(kTgThreads, 2)
 traj_grad_kernel(ForceParams P, TgParams T)
 {
@@ -802,6 +802,7 @@ traj_grad_kernel(ForceParams P, TgParams T)
     const int nb = P.n_b, st = blockDim.x, np = T.n_par, W = 6 + 6 * np;
     double *fd = (double *)(sm + Ly.total) + threadIdx.x;
     double *gf = fd + (size_t)nb * st, *gs = gf + (size_t)nb * st;
+    double *keep = gs + (size_t)nb * st;  // KEEP: NGMAX (NEMAX + 2) slots per thread
     const int tl = threadIdx.x % kTgLanes;
     const int a = tl / kTgSub, jsub = tl % kTgSub;  // axis slot, sub-lane
     const bool axis = a < 3;
@@ -830,10 +831,12 @@ traj_grad_kernel(ForceParams P, TgParams T)
         if (valid && axis && jsub == 0) {
             dst[a] = x;
             dst[3 + a] = u;
-            for (int k = 0; k < np; k++) {
-                dst[6 + a * np + k] = Tx[k];
-                dst[6 + 3 * np + a * np + k] = Tv[k];
-            }
+#pragma unroll
+            for (int k = 0; k < kTgMaxPar; k++)  // compile-time indices keep Tx, Tv in registers
+                if (k < np) {
+                    dst[6 + a * np + k] = Tx[k];
+                    dst[6 + 3 * np + a * np + k] = Tv[k];
+                }
         }
     };
     // a particle already beyond r_escape stopped in an earlier call (the sum
@@ -858,8 +861,8 @@ traj_grad_kernel(ForceParams P, TgParams T)
             gs[b * st] = 0.0;
         }
         double gBG;
-        const RedOut o = reduced_adjoint_point<NGMAX, NEMAX, EXACT, PAD, kTgSub>(
-            P, S, P.pol, act ? u : 0.0, act ? x : 0.0, Bg, fd, st, gf, gs, gBG, jsub);
+        const RedOut o = reduced_adjoint_point<NGMAX, NEMAX, EXACT, PAD, kTgSub, KEEP>(
+            P, S, P.pol, act ? u : 0.0, act ? x : 0.0, Bg, fd, st, gf, gs, gBG, jsub, keep);
         if (act) {
             F = o.F;
             R = o.R;
@@ -889,7 +892,7 @@ traj_grad_kernel(ForceParams P, TgParams T)
         if (act) {
             const double acc = __ddiv_rn(F, T.mass);
             u = __dadd_rn(u, __dmul_rn(acc, T.dt));
-            if (T.kicks) u = __dadd_rn(u, kick[a]);
+            if (T.kicks) u = __dadd_rn(u, (a == 0) ? kick[0] : (a == 1) ? kick[1] : kick[2]);  // no run-time index
             x = __dadd_rn(x, __dmul_rn(u, T.dt));
             const double im = T.dt / T.mass;
 #pragma unroll
@@ -1074,17 +1077,28 @@ int launch_reduced_adjoint(const ForceParams &P, double *grad, cudaStream_t st)
 template <class C, int PAD>
 int launch_traj_grad(const ForceParams &P, const TgParams &T, cudaStream_t st)
 {
-    auto kern = traj_grad_kernel<C::ng, C::ne, C::exact, PAD>;
-    RedLayout<C::ng, C::ne> Ly;
-    Ly.build(P.n_b, true);
-    const size_t sb = Ly.total + sizeof(double) * 3 * P.n_b * kTgThreads;
-    if (sb > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb);
-        if (mm_cuda_check(e, "cudaFuncSetAttribute")) return -3;
-    }
     const long long gx = ((long long)kTgLanes * T.n_particles + kTgThreads - 1) / kTgThreads;
-    kern<<<(unsigned)gx, kTgThreads, sb, st>>>(P, T);
-    return mm_cuda_check(cudaGetLastError(), "traj_grad_kernel launch") ? -3 : 0;
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    // an ensemble of at most one CTA per SM keeps each ground state's rate sums
+    // from the adjoint point's first pass in shared memory (the second pass
+    // then skips the rates); larger ensembles keep two CTAs per SM instead
+    auto go = [&](auto keepc) -> int {
+        constexpr bool KEEP = decltype(keepc)::value;
+        auto kern = traj_grad_kernel<C::ng, C::ne, C::exact, PAD, KEEP>;
+        RedLayout<C::ng, C::ne> Ly;
+        Ly.build(P.n_b, true);
+        const size_t sb = Ly.total + sizeof(double) * (3 * (size_t)P.n_b + (KEEP ? C::ng * (C::ne + 2) : 0)) * kTgThreads;
+        if (sb > 48 * 1024) {
+            cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb);
+            if (mm_cuda_check(e, "cudaFuncSetAttribute")) return -3;
+        }
+        kern<<<(unsigned)gx, kTgThreads, sb, st>>>(P, T);
+        return mm_cuda_check(cudaGetLastError(), "traj_grad_kernel launch") ? -3 : 0;
+    };
+    if (gx <= nsm) return go(std::true_type{});
+    return go(std::false_type{});
 }
 
 template <class C>

@@ -475,22 +475,32 @@ __device__ Out3 force3d_point(const Force3Params &P, Smem3<NGM, NEM, TH> &S,
     for (int e = 0; e < NEM; e++) Racc[e] = 0.0;
     if (t < n_g) {
         const double Eg = W.Esg[t];
+        // per-state constants of the beam loop, in registers: the transition
+        // frequencies and |x|^2 (0 below the 1e-15 cut, which adds an exact 0)
+        double om[NEM], d2m[NEM][3];
+#pragma unroll
+        for (int e = 0; e < NEM; e++) {
+            om[e] = (e < n_e) ? __dsub_rn(W.Ese[e], Eg) : 0.0;
+#pragma unroll
+            for (int q = 0; q < 3; q++) {
+                const double d2 = (e < n_e) ? W.dsq[(e * 3 + q) * NGM + t] : 0.0;
+                d2m[e][q] = (d2 >= 1e-15) ? d2 : 0.0;
+            }
+        }
         for (int b = 0; b < n_b; b++) {
             const double fd = __dadd_rn(S.freq[b], W.bm[b][0]);
             const double se = W.bm[b][1];
+            const double w0 = W.bm[b][2], w1 = W.bm[b][3], w2 = W.bm[b][4];
             double Qb = 0.0;
 #pragma unroll
             for (int e = 0; e < NEM; e++) {
                 if (e < n_e) {
-                    const double om = __dsub_rn(W.Ese[e], Eg);
-                    const double de = __dmul_rn(__dsub_rn(fd, om), MM_TWO_PI);
+                    const double de = __dmul_rn(__dsub_rn(fd, om[e]), MM_TWO_PI);
                     const double L = gh2 * mm_rcp(fma(de, de, gh2));
                     double ws = 0.0;
-#pragma unroll
-                    for (int q = 0; q < 3; q++) {
-                        const double d2 = W.dsq[(e * 3 + q) * NGM + t];
-                        if (d2 >= 1e-15) ws = fma(W.bm[b][2 + q], d2, ws);
-                    }
+                    ws = fma(w0, d2m[e][0], ws);
+                    ws = fma(w1, d2m[e][1], ws);
+                    ws = fma(w2, d2m[e][2], ws);
                     const double rb = ws * L * se;
                     Racc[e] += rb;
                     Qb += rb;

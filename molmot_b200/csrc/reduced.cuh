@@ -623,12 +623,17 @@ __device__ __forceinline__ double red_lane_sum(double x)
     return x;
 }
 
-template <int NGMAX, int NEMAX, bool EXACT, int PAD, int NL = 1>
+template <int NGMAX, int NEMAX, bool EXACT, int PAD, int NL = 1, bool KEEP = false>
 __device__ __forceinline__ RedOut reduced_adjoint_point(const ForceParams &P, const RedView &S,
                                                         const int32_t *pol, double v, double z,
                                                         double Bgrad, double *fd, int stride,
-                                                        double *gf, double *gs, double &gBG, int j = 0)
+                                                        double *gf, double *gs, double &gBG, int j = 0,
+                                                        double *keep = nullptr)
 {
+    // KEEP: the first pass stores each ground state's sums (R[g,e] for e <
+    // NEMAX, f_g, s_g) in this thread's slots keep[(g (NEMAX + 2) + i) stride],
+    // and the second pass reads them instead of recomputing the rates (the
+    // same bits: the same operations on the same inputs)
     const int n_g = EXACT ? NGMAX : P.n_g;
     const int n_e = EXACT ? NEMAX : P.n_e;
     RateCtx<NEMAX> C;
@@ -656,6 +661,13 @@ __device__ __forceinline__ RedOut reduced_adjoint_point(const ForceParams &P, co
     for (int g = j; g < n_g; g += NL) {
         double Re[NEMAX], f, s;
         reduced_rates<NEMAX, PAD, true>(S, g, C, gh2, Re, f, s);
+        if constexpr (KEEP) {
+            double *kg = keep + (size_t)g * (NEMAX + 2) * stride;
+#pragma unroll
+            for (int e = 0; e < NEMAX; e++) kg[e * stride] = Re[e];
+            kg[NEMAX * stride] = f;
+            kg[(NEMAX + 1) * stride] = s;
+        }
         double rt = 0.0;
 #pragma unroll
         for (int e = 0; e < NEMAX; e++) rt += Re[e];
@@ -737,7 +749,15 @@ __device__ __forceinline__ RedOut reduced_adjoint_point(const ForceParams &P, co
     const double inrm = in, Fin = F * in;
     for (int g = j; g < n_g; g += NL) {
         double Re[NEMAX], f, s;
-        reduced_rates<NEMAX, PAD, true>(S, g, C, gh2, Re, f, s);
+        if constexpr (KEEP) {
+            const double *kg = keep + (size_t)g * (NEMAX + 2) * stride;
+#pragma unroll
+            for (int e = 0; e < NEMAX; e++) Re[e] = kg[e * stride];
+            f = kg[NEMAX * stride];
+            s = kg[(NEMAX + 1) * stride];
+        } else {
+            reduced_rates<NEMAX, PAD, true>(S, g, C, gh2, Re, f, s);
+        }
         double rt = 0.0, yg = 0.0;
 #pragma unroll
         for (int e = 0; e < NEMAX; e++) {
