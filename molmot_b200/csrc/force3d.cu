@@ -108,6 +108,16 @@ __device__ __forceinline__ double gsum16(double x)
 }
 
 
+// 1/sqrt(x) for x >= 0: the Newton-refined hardware approximation
+// (mm_rsqrt, within an ulp) for normal x, IEEE sqrt and division otherwise
+// (0, subnormal, inf).  The eigensolver's rotations and norms use it in place
+// of a square root and one or two divisions.
+__device__ __forceinline__ double rsqrt_any(double x)
+{
+    if (x >= 2.2250738585072014e-308 && x <= 1.0e300) return mm_rsqrt(x);
+    return 1.0 / sqrt(x);
+}
+
 template <int NGM, int NEM, int TH>
 __device__ void load_consts3(const Force3Params &P, int set, Smem3<NGM, NEM, TH> &S)
 {
@@ -184,11 +194,14 @@ __device__ bool hermitian_eigen(GroupT &W, int t, int n)
         const double rest = gsum16((t > k + 1) ? xr * xr + xi * xi : 0.0);
         const bool act = rest > 0.0;  // the same on the 16 lanes of a group
         const double x0r = W.Hre[(k + 1) * LDH + k], x0i = W.Him[(k + 1) * LDH + k];
-        const double a0 = sqrt(x0r * x0r + x0i * x0i);
-        const double nx = sqrt(fma(a0, a0, rest));
-        const double phr = (a0 > 0.0) ? x0r / a0 : 1.0, phi = (a0 > 0.0) ? x0i / a0 : 0.0;
+        const double a0s = x0r * x0r + x0i * x0i;
+        const double ia0 = rsqrt_any(a0s);
+        const double a0 = (a0s > 0.0) ? a0s * ia0 : 0.0;  // |x0|
+        const double nxs = fma(a0, a0, rest);
+        const double nx = (nxs > 0.0) ? nxs * rsqrt_any(nxs) : 0.0;
+        const double phr = (a0 > 0.0) ? x0r * ia0 : 1.0, phi = (a0 > 0.0) ? x0i * ia0 : 0.0;
         // v = x - alpha e1 = x + ph nx e1, normalised: |v|^2 = rest + (a0 + nx)^2
-        const double iv = act ? 1.0 / sqrt(fma(a0 + nx, a0 + nx, rest)) : 0.0;
+        const double iv = act ? rsqrt_any(fma(a0 + nx, a0 + nx, rest)) : 0.0;
         if (t > k && row) {
             double vr = xr, vi = xi;
             if (t == k + 1) { vr = phr * (a0 + nx); vi = phi * (a0 + nx); }
@@ -252,10 +265,12 @@ __device__ bool hermitian_eigen(GroupT &W, int t, int n)
         di[i] = ci;
         if (i + 1 < n) {
             const double hr = W.Hre[(i + 1) * LDH + i], hi = W.Him[(i + 1) * LDH + i];
-            const double a = sqrt(hr * hr + hi * hi);
+            const double as = hr * hr + hi * hi;
+            const double ia = rsqrt_any(as);
+            const double a = (as > 0.0) ? as * ia : 0.0;
             if (i == t) el = a;
             if (a > 0.0) {
-                const double ur = hr / a, ui = hi / a;
+                const double ur = hr * ia, ui = hi * ia;
                 const double nr = cr * ur - ci * ui;
                 ci = cr * ui + ci * ur;
                 cr = nr;
@@ -297,16 +312,18 @@ __device__ bool hermitian_eigen(GroupT &W, int t, int n)
             for (int i = m - 1; i >= l; i--) {
                 const double ei = __shfl_sync(gmask, el, i, 16), dii = __shfl_sync(gmask, dl, i, 16);
                 const double f = s * ei, b = c * ei;
-                r = sqrt(fma(f, f, g * g));
-                if (t == i + 1) el = r;
-                if (r == 0.0) {  // deflation: the rotation vanished
-                    if (t == i + 1) dl -= p;
+                const double rs = fma(f, f, g * g);
+                if (rs == 0.0) {  // deflation: the rotation vanished
+                    if (t == i + 1) { el = 0.0; dl -= p; }
                     if (t == m) el = 0.0;
                     defl = true;
                     break;
                 }
-                s = f / r;
-                c = g / r;
+                const double ir = rsqrt_any(rs);
+                r = rs * ir;
+                if (t == i + 1) el = r;
+                s = f * ir;
+                c = g * ir;
                 g = dnext - p;
                 r = (dii - g) * s + 2.0 * c * b;
                 p = s * r;
