@@ -789,6 +789,7 @@ constexpr int kTgMaxPar = MM_TGRAD_MAX_PAR;
 constexpr int kTgThreads = 128;
 constexpr int kTgSub = 1;             // lanes per axis (each takes every kTgSub-th ground state)
 constexpr int kTgLanes = 4 * kTgSub;  // lanes per particle: x, y, z and an idle slot
+constexpr int kTgBofs = (MM_MAX_BEAMS + 4) / 4 * 4;  // beam offsets (ints), a multiple of 4
 
 template <int NGMAX, int NEMAX, bool EXACT, int PAD, bool KEEP>
 __global__ void __launch_bounds__(kTgThreads, 2)
@@ -803,6 +804,26 @@ traj_grad_kernel(ForceParams P, TgParams T)
     double *fd = (double *)(sm + Ly.total) + threadIdx.x;
     double *gf = fd + (size_t)nb * st, *gs = gf + (size_t)nb * st;
     double *keep = gs + (size_t)nb * st;  // KEEP: NGMAX (NEMAX + 2) slots per thread
+    // KEEP: the triples in beam-major order (reduced_adjoint_point's gradient pass)
+    // (the same address on every thread: after the per-thread regions, which
+    // are counted from the shared base, not from this thread's slot)
+    int *bofs = (int *)((double *)(sm + Ly.total) + (size_t)(3 * nb + NGMAX * (NEMAX + 2)) * st);
+    int *bidx = bofs + kTgBofs;
+    if constexpr (KEEP) {
+        if (threadIdx.x == 0) {
+            const TripD *tr = (const TripD *)S.trip;
+            int k = 0;
+            for (int b = 0; b < nb; b++) {
+                bofs[b] = k;
+                for (int g = 0; g < P.n_g; g++)
+                    for (int e = 0; e < P.n_e; e++)
+                        for (int i = S.offs[g * NEMAX + e]; i < S.offs[g * NEMAX + e + 1]; i++)
+                            if (!tr[i].pad && tr[i].b == b) bidx[k++] = i | (g << 16) | (e << 24);
+            }
+            bofs[nb] = k;
+        }
+        __syncthreads();
+    }
     const int tl = threadIdx.x % kTgLanes;
     const int a = tl / kTgSub, jsub = tl % kTgSub;  // axis slot, sub-lane
     const bool axis = a < 3;
@@ -862,7 +883,7 @@ traj_grad_kernel(ForceParams P, TgParams T)
         }
         double gBG;
         const RedOut o = reduced_adjoint_point<NGMAX, NEMAX, EXACT, PAD, kTgSub, KEEP>(
-            P, S, P.pol, act ? u : 0.0, act ? x : 0.0, Bg, fd, st, gf, gs, gBG, jsub, keep);
+            P, S, P.pol, act ? u : 0.0, act ? x : 0.0, Bg, fd, st, gf, gs, gBG, jsub, keep, bofs, bidx);
         if (act) {
             F = o.F;
             R = o.R;
@@ -1089,7 +1110,9 @@ int launch_traj_grad(const ForceParams &P, const TgParams &T, cudaStream_t st)
         auto kern = traj_grad_kernel<C::ng, C::ne, C::exact, PAD, KEEP>;
         RedLayout<C::ng, C::ne> Ly;
         Ly.build(P.n_b, true);
-        const size_t sb = Ly.total + sizeof(double) * (3 * (size_t)P.n_b + (KEEP ? C::ng * (C::ne + 2) : 0)) * kTgThreads;
+        const size_t slots = (size_t)C::ng * C::ne * ((P.n_b + kRedPad - 1) / kRedPad * kRedPad);
+        const size_t sb = Ly.total + sizeof(double) * (3 * (size_t)P.n_b + (KEEP ? C::ng * (C::ne + 2) : 0)) * kTgThreads +
+                          (KEEP ? sizeof(int) * (kTgBofs + slots) : 0);
         if (sb > 48 * 1024) {
             cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb);
             if (mm_cuda_check(e, "cudaFuncSetAttribute")) return -3;

@@ -628,12 +628,19 @@ __device__ __forceinline__ RedOut reduced_adjoint_point(const ForceParams &P, co
                                                         const int32_t *pol, double v, double z,
                                                         double Bgrad, double *fd, int stride,
                                                         double *gf, double *gs, double &gBG, int j = 0,
-                                                        double *keep = nullptr)
+                                                        double *keep = nullptr, const int *bofs = nullptr,
+                                                        const int *bidx = nullptr)
 {
     // KEEP: the first pass stores each ground state's sums (R[g,e] for e <
     // NEMAX, f_g, s_g) in this thread's slots keep[(g (NEMAX + 2) + i) stride],
     // and the second pass reads them instead of recomputing the rates (the
-    // same bits: the same operations on the same inputs)
+    // same operations on the same inputs).  Its coefficients (alpha_ge, beta_g,
+    // gamma_g) then replace them, and the triples run beam by beam through
+    // the beam-major index (bofs[b] .. bofs[b + 1] into bidx, each entry
+    // i | g << 16 | e << 24): each beam's dF/dfreq_b and dF/ds0_b add up in
+    // registers and are stored once.  Ground-major, the shared-memory
+    // accumulators indexed by each triple's beam kept the compiler from
+    // overlapping consecutive triples (a store may alias the next load).
     const int n_g = EXACT ? NGMAX : P.n_g;
     const int n_e = EXACT ? NEMAX : P.n_e;
     RateCtx<NEMAX> C;
@@ -747,53 +754,104 @@ __device__ __forceinline__ RedOut reduced_adjoint_point(const ForceParams &P, co
     // second pass: per ground state coefficients, then the triples once more
     gBG = 0.0;
     const double inrm = in, Fin = F * in;
-    for (int g = j; g < n_g; g += NL) {
-        double Re[NEMAX], f, s;
-        if constexpr (KEEP) {
-            const double *kg = keep + (size_t)g * (NEMAX + 2) * stride;
+    if constexpr (KEEP) {
+        for (int g = j; g < n_g; g += NL) {
+            double *kg = keep + (size_t)g * (NEMAX + 2) * stride;
+            double Re[NEMAX];
 #pragma unroll
             for (int e = 0; e < NEMAX; e++) Re[e] = kg[e * stride];
-            f = kg[NEMAX * stride];
-            s = kg[(NEMAX + 1) * stride];
-        } else {
-            reduced_rates<NEMAX, PAD, true>(S, g, C, gh2, Re, f, s);
+            const double f = kg[NEMAX * stride], s = kg[(NEMAX + 1) * stride];
+            double rt = 0.0, yg = 0.0;
+#pragma unroll
+            for (int e = 0; e < NEMAX; e++) {
+                rt += Re[e];
+                yg = fma(S.brt[g * NEMAX + e], pi[e], yg);
+            }
+            const double inv = mm_rcp(rt);
+            const double phi = f * inv, w = (1.0 + s) * inv;
+            double Lam = 0.0;
+#pragma unroll
+            for (int e = 0; e < NEMAX; e++) Lam = fma(lam[e], Re[e] * inv, Lam);
+            const double yi = yg * inv;
+            const double common = -Lam - phi * inrm + w * Fin;
+#pragma unroll
+            for (int e = 0; e < NEMAX; e++) kg[e * stride] = yi * (lam[e] + common);  // alpha_ge
+            kg[NEMAX * stride] = yi * inrm;                                            // beta_g
+            kg[(NEMAX + 1) * stride] = -yi * Fin;                                      // gamma_g
         }
-        double rt = 0.0, yg = 0.0;
-#pragma unroll
-        for (int e = 0; e < NEMAX; e++) {
-            rt += Re[e];
-            yg = fma(S.brt[g * NEMAX + e], pi[e], yg);
-        }
-        const double inv = mm_rcp(rt);
-        const double phi = f * inv, w = (1.0 + s) * inv;
-        double Lam = 0.0;
-#pragma unroll
-        for (int e = 0; e < NEMAX; e++) Lam = fma(lam[e], Re[e] * inv, Lam);
-        const double yi = yg * inv;
-        const double beta = yi * inrm, gamma = -yi * Fin;
-        const double common = -Lam - phi * inrm + w * Fin;
-        const double Esg = fma(C.B, S.czd[g], S.E[g]);
-#pragma unroll
-        for (int e = 0; e < NEMAX; e++) {
-            const double alpha = yi * (lam[e] + common);
-            const int i0 = S.offs[g * NEMAX + e], i1 = S.offs[g * NEMAX + e + 1];
-            const double om = __dsub_rn(C.Ese[e], Esg);
-            const double dBde = -(S.zde[e] - P.zd[g]) * P.Gamma;  // d delta / dB
-            for (int i = i0; i < i1; i++) {
+        const double ggh = gh * P.geff;
+        for (int b = 0; b < P.n_b; b++) {
+            const double fdb = fd[b * stride];
+            double gfb = 0.0, gsb = 0.0;
+            for (int k = bofs[b]; k < bofs[b + 1]; k++) {
+                const int code = bidx[k];
+                const int i = code & 0xffff, g = (code >> 16) & 0xff, e = code >> 24;
+                if (NL > 1 && g % NL != j) continue;
                 const TripD tr = ((const TripD *)S.trip)[i];
-                if (tr.pad) continue;  // list padding
-                const int b = tr.b;
-                const double de = __dmul_rn(__dsub_rn(fd[b * stride], om), MM_TWO_PI);
+                const double *kg = keep + (size_t)g * (NEMAX + 2) * stride;
+                double alpha = kg[0], Ese = C.Ese[0];
+#pragma unroll
+                for (int ee = 1; ee < NEMAX; ee++)  // no run-time register index
+                    if (ee == e) { alpha = kg[ee * stride]; Ese = C.Ese[ee]; }
+                const double beta = kg[NEMAX * stride], gamma = kg[(NEMAX + 1) * stride];
+                const double om = __dsub_rn(Ese, fma(C.B, S.czd[g], S.E[g]));
+                const double de = __dmul_rn(__dsub_rn(fdb, om), MM_TWO_PI);
                 const double iden = mm_rcp1(fma(de, de, gh2));  // feeds the gradient only
                 const double L = gh2 * iden;
                 const double dLd = -2.0 * de * L * iden;  // dL / d delta
-                const double q = fma(alpha + beta * tr.hk, tr.c1, gamma * tr.c2);
-                gf[b * stride] = fma(q * dLd, MM_TWO_PI, gf[b * stride]);
+                const double ab = alpha + beta * tr.hk;
+                const double q = fma(ab, tr.c1, gamma * tr.c2);
+                gfb = fma(q * dLd, MM_TWO_PI, gfb);
                 // d(c1, c2)/ds0_b with d2 = c2 / s0_b written out: c1 = ((Gamma/2) s0 d2) Geff
                 const double d2 = S.d2t[i];
-                const double qs = fma((alpha + beta * tr.hk) * gh * P.geff, d2, gamma * d2);
-                gs[b * stride] = fma(qs, L, gs[b * stride]);
+                gsb = fma(fma(ab * ggh, d2, gamma * d2), L, gsb);
+                const double dBde = -(S.zde[e] - P.zd[g]) * P.Gamma;  // d delta / dB
                 gBG = fma(q * dLd, dBde, gBG);
+            }
+            gf[b * stride] += gfb;
+            gs[b * stride] += gsb;
+        }
+    } else {
+        for (int g = j; g < n_g; g += NL) {
+            double Re[NEMAX], f, s;
+            reduced_rates<NEMAX, PAD, true>(S, g, C, gh2, Re, f, s);
+            double rt = 0.0, yg = 0.0;
+#pragma unroll
+            for (int e = 0; e < NEMAX; e++) {
+                rt += Re[e];
+                yg = fma(S.brt[g * NEMAX + e], pi[e], yg);
+            }
+            const double inv = mm_rcp(rt);
+            const double phi = f * inv, w = (1.0 + s) * inv;
+            double Lam = 0.0;
+#pragma unroll
+            for (int e = 0; e < NEMAX; e++) Lam = fma(lam[e], Re[e] * inv, Lam);
+            const double yi = yg * inv;
+            const double beta = yi * inrm, gamma = -yi * Fin;
+            const double common = -Lam - phi * inrm + w * Fin;
+            const double Esg = fma(C.B, S.czd[g], S.E[g]);
+#pragma unroll
+            for (int e = 0; e < NEMAX; e++) {
+                const double alpha = yi * (lam[e] + common);
+                const int i0 = S.offs[g * NEMAX + e], i1 = S.offs[g * NEMAX + e + 1];
+                const double om = __dsub_rn(C.Ese[e], Esg);
+                const double dBde = -(S.zde[e] - P.zd[g]) * P.Gamma;  // d delta / dB
+                for (int i = i0; i < i1; i++) {
+                    const TripD tr = ((const TripD *)S.trip)[i];
+                    if (tr.pad) continue;  // list padding
+                    const int b = tr.b;
+                    const double de = __dmul_rn(__dsub_rn(fd[b * stride], om), MM_TWO_PI);
+                    const double iden = mm_rcp1(fma(de, de, gh2));  // feeds the gradient only
+                    const double L = gh2 * iden;
+                    const double dLd = -2.0 * de * L * iden;  // dL / d delta
+                    const double q = fma(alpha + beta * tr.hk, tr.c1, gamma * tr.c2);
+                    gf[b * stride] = fma(q * dLd, MM_TWO_PI, gf[b * stride]);
+                    // d(c1, c2)/ds0_b with d2 = c2 / s0_b written out: c1 = ((Gamma/2) s0 d2) Geff
+                    const double d2 = S.d2t[i];
+                    const double qs = fma((alpha + beta * tr.hk) * gh * P.geff, d2, gamma * d2);
+                    gs[b * stride] = fma(qs, L, gs[b * stride]);
+                    gBG = fma(q * dLd, dBde, gBG);
+                }
             }
         }
     }
