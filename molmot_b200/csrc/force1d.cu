@@ -803,11 +803,11 @@ traj_grad_kernel(ForceParams P, TgParams T)
     const int nb = P.n_b, st = blockDim.x, np = T.n_par, W = 6 + 6 * np;
     double *fd = (double *)(sm + Ly.total) + threadIdx.x;
     double *gf = fd + (size_t)nb * st, *gs = gf + (size_t)nb * st;
-    double *keep = gs + (size_t)nb * st;  // KEEP: NGMAX (NEMAX + 2) slots per thread
+    double *keep = gs + (size_t)nb * st;  // KEEP: NGMAX kKeepSlots slots per thread
     // KEEP: the triples in beam-major order (reduced_adjoint_point's gradient pass)
     // (the same address on every thread: after the per-thread regions, which
     // are counted from the shared base, not from this thread's slot)
-    int *bofs = (int *)((double *)(sm + Ly.total) + (size_t)(3 * nb + NGMAX * (NEMAX + 2)) * st);
+    int *bofs = (int *)((double *)(sm + Ly.total) + (size_t)(3 * nb + NGMAX * kKeepSlots<NEMAX>) * st);
     int *bidx = bofs + kTgBofs;
     if constexpr (KEEP) {
         if (threadIdx.x == 0) {
@@ -1111,7 +1111,7 @@ int launch_traj_grad(const ForceParams &P, const TgParams &T, cudaStream_t st)
         RedLayout<C::ng, C::ne> Ly;
         Ly.build(P.n_b, true);
         const size_t slots = (size_t)C::ng * C::ne * ((P.n_b + kRedPad - 1) / kRedPad * kRedPad);
-        const size_t sb = Ly.total + sizeof(double) * (3 * (size_t)P.n_b + (KEEP ? C::ng * (C::ne + 2) : 0)) * kTgThreads +
+        const size_t sb = Ly.total + sizeof(double) * (3 * (size_t)P.n_b + (KEEP ? C::ng * kKeepSlots<C::ne> : 0)) * kTgThreads +
                           (KEEP ? sizeof(int) * (kTgBofs + slots) : 0);
         if (sb > 48 * 1024) {
             cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb);

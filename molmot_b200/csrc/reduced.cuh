@@ -42,6 +42,12 @@
 // the kernel, which then holds one loop form only.
 constexpr int kRedPad = 4;
 
+// Slots per ground state of reduced_adjoint_point's KEEP buffer: the rate sums
+// (R[g,e] for e < NEMAX, f_g, s_g), later alpha_ge, beta_g, gamma_g, then the
+// transition offsets omega_ge = E_e(B) - E_g(B).
+template <int NEMAX>
+constexpr int kKeepSlots = 2 * NEMAX + 2;
+
 // One active (ground g, beam b, excited e) triple: 32 bytes.
 struct TripR {
     float u0;    // (freq_b - (E_e - E_g)) 2pi/(Gamma/2)  (FP64, rounded once)
@@ -632,7 +638,7 @@ __device__ __forceinline__ RedOut reduced_adjoint_point(const ForceParams &P, co
                                                         const int *bidx = nullptr)
 {
     // KEEP: the first pass stores each ground state's sums (R[g,e] for e <
-    // NEMAX, f_g, s_g) in this thread's slots keep[(g (NEMAX + 2) + i) stride],
+    // NEMAX, f_g, s_g) in this thread's slots keep[(g kKeepSlots + i) stride],
     // and the second pass reads them instead of recomputing the rates (the
     // same operations on the same inputs).  Its coefficients (alpha_ge, beta_g,
     // gamma_g) then replace them, and the triples run beam by beam through
@@ -669,7 +675,7 @@ __device__ __forceinline__ RedOut reduced_adjoint_point(const ForceParams &P, co
         double Re[NEMAX], f, s;
         reduced_rates<NEMAX, PAD, true>(S, g, C, gh2, Re, f, s);
         if constexpr (KEEP) {
-            double *kg = keep + (size_t)g * (NEMAX + 2) * stride;
+            double *kg = keep + (size_t)g * kKeepSlots<NEMAX> * stride;
 #pragma unroll
             for (int e = 0; e < NEMAX; e++) kg[e * stride] = Re[e];
             kg[NEMAX * stride] = f;
@@ -756,7 +762,7 @@ __device__ __forceinline__ RedOut reduced_adjoint_point(const ForceParams &P, co
     const double inrm = in, Fin = F * in;
     if constexpr (KEEP) {
         for (int g = j; g < n_g; g += NL) {
-            double *kg = keep + (size_t)g * (NEMAX + 2) * stride;
+            double *kg = keep + (size_t)g * kKeepSlots<NEMAX> * stride;
             double Re[NEMAX];
 #pragma unroll
             for (int e = 0; e < NEMAX; e++) Re[e] = kg[e * stride];
@@ -778,6 +784,9 @@ __device__ __forceinline__ RedOut reduced_adjoint_point(const ForceParams &P, co
             for (int e = 0; e < NEMAX; e++) kg[e * stride] = yi * (lam[e] + common);  // alpha_ge
             kg[NEMAX * stride] = yi * inrm;                                            // beta_g
             kg[(NEMAX + 1) * stride] = -yi * Fin;                                      // gamma_g
+            const double Esg = fma(C.B, S.czd[g], S.E[g]);
+#pragma unroll
+            for (int e = 0; e < NEMAX; e++) kg[(NEMAX + 2 + e) * stride] = __dsub_rn(C.Ese[e], Esg);  // omega_ge
         }
         const double ggh = gh * P.geff;
         for (int b = 0; b < P.n_b; b++) {
@@ -788,13 +797,9 @@ __device__ __forceinline__ RedOut reduced_adjoint_point(const ForceParams &P, co
                 const int i = code & 0xffff, g = (code >> 16) & 0xff, e = code >> 24;
                 if (NL > 1 && g % NL != j) continue;
                 const TripD tr = ((const TripD *)S.trip)[i];
-                const double *kg = keep + (size_t)g * (NEMAX + 2) * stride;
-                double alpha = kg[0], Ese = C.Ese[0];
-#pragma unroll
-                for (int ee = 1; ee < NEMAX; ee++)  // no run-time register index
-                    if (ee == e) { alpha = kg[ee * stride]; Ese = C.Ese[ee]; }
+                const double *kg = keep + (size_t)g * kKeepSlots<NEMAX> * stride;
+                const double alpha = kg[e * stride], om = kg[(NEMAX + 2 + e) * stride];
                 const double beta = kg[NEMAX * stride], gamma = kg[(NEMAX + 1) * stride];
-                const double om = __dsub_rn(Ese, fma(C.B, S.czd[g], S.E[g]));
                 const double de = __dmul_rn(__dsub_rn(fdb, om), MM_TWO_PI);
                 const double iden = mm_rcp1(fma(de, de, gh2));  // feeds the gradient only
                 const double L = gh2 * iden;
