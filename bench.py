@@ -841,12 +841,12 @@ def main():
     d2h = pinned_F.numel() * 8
 
     def e2e_step():
-        # parameters and grid axes host->device, maps device->host in 256-set
+        # parameters and grid axes host->device, maps device->host in 64-set
         # chunks whose copies overlap the next chunk's computation
         b2 = BeamSets(*params_h)
         vv = torch.as_tensor(v_h).to(dev)
         zz = torch.as_tensor(z_h).to(dev)
-        return force_maps_to_host(pack, b2, vv, zz, out=pinned_F, precision="fp32", chunk_sets=256)
+        return force_maps_to_host(pack, b2, vv, zz, out=pinned_F, precision="fp32", chunk_sets=64)
 
     for _ in range(max(1, args.warmup)):
         e2e_step()
@@ -901,7 +901,7 @@ def main():
                 "flops_per_point": {"fp64": f64_32, "fp32": f32_32}}
         e2e = {"value": total / (ms_e2e * 1e-3), "unit": "force evals/s",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "ms_per_step": ms_e2e,
-               "api": "engine.force_maps_to_host, 256-set chunks"}
+               "api": "engine.force_maps_to_host, 64-set chunks"}
         details = {"bench_details": {
             "plain_fp64": plain, "fp64_reduced": red64, "accuracy": accuracy, "secondary": secondary,
             "roofline": dict(roof, hbm=hbm_figure(8 * n_pts, ms32),

@@ -228,15 +228,18 @@ _COPY_STREAMS = {}
 
 
 def force_maps_to_host(pack: MoleculePack, beams: BeamSets, v, z, out=None, *, precision="fp32",
-                       hbar=None, chunk_sets: int = 256, sync: bool = True):
+                       hbar=None, chunk_sets: int = 64, sync: bool = True):
     """Force maps F[n_sets, nv, nz] of every parameter set (grid layout) in
     host memory.
 
     The sets are computed in chunks of ``chunk_sets`` on the current stream,
     alternating between two device buffers; each chunk's device->host copy runs
     on a second stream while the next chunk is computed, so the transfer of
-    the maps hides the computation.  ``out``: a host float64 tensor of that
-    shape (page-locked for overlapped copies; allocated page-locked if None).
+    the maps hides the computation.  Only the first chunk's computation is
+    not hidden: 64-set chunks (the default) took 39.0 ms for 4096 SrOH sets x
+    256 x 256 against 40.2 ms with 256-set chunks, where one 2.15 GB copy
+    alone takes 37.6 ms.  ``out``: a host float64 tensor of that shape
+    (page-locked for overlapped copies; allocated page-locked if None).
     With sync=False the call returns once everything is enqueued and the maps
     are complete when the current stream reaches that point.
     """
